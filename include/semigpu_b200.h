@@ -1,0 +1,126 @@
+/* semigpu_b200 — C ABI of the B200 MNDO SCF engine.
+ *
+ * Plain pointers and sizes only.  Every call returns an int status: 0 on success, < 0 on an
+ * error (see SGB_E_*), and sgb_last_error() gives the message.  A context owns one CUDA stream
+ * on one device; molecule and batch handles own their device memory; all host buffers are the
+ * caller's.  Calls on one context are not thread-safe (one host thread per context, as the
+ * reference's single-threaded driver).
+ *
+ * Units follow the reference: coordinates in Angstrom on input (converted to bohr with
+ * 1.8897259886, mymath.h:84-87), energies and matrix elements in eV.  Matrices are packed
+ * lower triangles, element (i,j) with i >= j at i*(i+1)/2 + j (mymemory.cpp:369-371); the AO
+ * order is atoms in input order, one s AO for H and s, px, py, pz for C, N, O
+ * (atomicOrbitals.cpp:76-119).  Reference paths are under src/common/ of
+ * LuisAlfredoNu/semiGPU.
+ */
+#ifndef SEMIGPU_B200_H
+#define SEMIGPU_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------------- */
+#define SGB_OK 0
+#define SGB_E_ARG -1          /* invalid argument (null pointer, bad size, bad enum)        */
+#define SGB_E_ELEMENT -2      /* element without MNDO parameters (only H, C, N, O)           */
+#define SGB_E_CUDA -3         /* CUDA runtime error (message in sgb_last_error)              */
+#define SGB_E_NOMEM -4        /* device allocation failed or over the context's HBM budget  */
+#define SGB_E_STATE -5        /* stage called out of order (e.g. Hcore before integrals)     */
+#define SGB_E_UNSUPPORTED -6  /* size outside what this build handles                        */
+#define SGB_E_EIG 1           /* SCF stopped: eigensolver did not converge (as LAPACK info>0)*/
+#define SGB_E_NAN 2           /* SCF stopped: non-finite energy                              */
+
+/* ---- matrices that can be read back ----------------------------------------------------- */
+#define SGB_BLOCKS 0  /* integral blocks, the reference's ragged [A][B<=A] array flattened   */
+#define SGB_HCORE 1   /* packed Hcore                                                        */
+#define SGB_FOCK 2    /* packed Fock matrix of the last SCF step                             */
+#define SGB_DENSITY 3 /* packed density matrix of the last SCF step                          */
+#define SGB_EIGVAL 4  /* nao eigenvalues of the last eigensolve, ascending                   */
+#define SGB_EIGVEC 5  /* nao x nao eigenvectors, column-major (column k = vector k), the    */
+                      /* layout of SCFCalculation::eigenVec                                  */
+
+typedef struct sgb_ctx sgb_ctx;
+typedef struct sgb_mol sgb_mol;
+typedef struct sgb_batch sgb_batch;
+
+typedef struct {
+  double e_el;    /* electronic energy (SCFCalculation::finalEnergy)                     */
+  int n_iter;     /* SCF steps taken                                                      */
+  int converged;  /* |dE| < tol reached (SCFCalculation::energyConverge)                  */
+  int status;     /* SGB_OK, SGB_E_EIG or SGB_E_NAN                                        */
+} sgb_scf_result;
+
+/* ---- context ---------------------------------------------------------------------------- */
+/* Binds a device, loads the MNDO tables, creates the stream.  hbm_budget_bytes = 0: no limit
+ * beyond the device's own. */
+int sgb_ctx_create(int device, size_t hbm_budget_bytes, sgb_ctx **out);
+int sgb_ctx_destroy(sgb_ctx *ctx);
+int sgb_ctx_synchronize(sgb_ctx *ctx);
+const char *sgb_last_error(const sgb_ctx *ctx);
+const char *sgb_status_string(int status);
+/* Bytes of device memory currently held by the context's molecules and batches. */
+size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
+
+/* ---- one molecule: the reference's stage API ------------------------------------------- */
+/* Replaces ReadXYZFile output handling + ListAtomicOrbitals::SetOrbitals
+ * (atomicOrbitals.cpp:76-119) + TwoCenterIntegral::Alloc4AllTwoCenterIntegral
+ * (twocenterintegral.cpp:55-107): validates the elements, builds the AO table and allocates
+ * integral blocks, Hcore, SCF matrices on the device.  Z: natoms atomic numbers; xyz:
+ * natoms*3 Cartesian coordinates in Angstrom. */
+int sgb_mol_create(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, sgb_mol **out);
+int sgb_mol_destroy(sgb_mol *mol);
+/* nao (ListAtomicOrbitals::size), nocc (DensityMatrix::NumberOfElectrons/2), integral
+ * doubles. */
+int sgb_mol_info(const sgb_mol *mol, int *natoms, int *nao, int *nocc, long long *nblocks);
+/* Replaces TwoCenterIntegral::ComputeAllTwoCenterIntegral + To_device
+ * (twocenterintegral.cpp:229-279, 23-53). */
+int sgb_two_center(sgb_ctx *ctx, sgb_mol *mol);
+/* Replaces Hcore::ComputeMatrix (hcore.cpp:104-124). */
+int sgb_hcore(sgb_ctx *ctx, sgb_mol *mol);
+/* Replaces SCFCalculation::AllocSCFData + ComputeSCF (scfcalculation.cpp:29-146) with the
+ * energy threshold (hard-coded 5e-3 eV at scfcalculation.cpp:77) and the step cap (100, :74)
+ * as arguments.  energies (optional, max_iter+1 doubles) receives E_0 .. E_n_iter. */
+int sgb_scf(sgb_ctx *ctx, sgb_mol *mol, double tol, int max_iter, sgb_scf_result *result,
+            double *energies);
+/* Replaces CoreCoreRepulsion::ComputeRepulsion (corecorerepulsion.cpp:12-41). */
+int sgb_core_core(sgb_ctx *ctx, sgb_mol *mol, double *e_cc);
+/* Replaces FockMatrix::ComputeMatrix (fockmatrix.cpp:32-53) followed by
+ * ElectronicEnergy::ComputeEnergy (electronicenergy.cpp:12-36) for a caller-given packed
+ * density P: F = Hcore + G(P) into F (packed, host), E_el into *e_el (may be NULL). */
+int sgb_fock(sgb_ctx *ctx, sgb_mol *mol, const double *P, double *F, double *e_el);
+/* Copies one of SGB_BLOCKS .. SGB_EIGVEC to host memory (sizes: see sgb_mol_info; packed
+ * matrices nao*(nao+1)/2, SGB_EIGVAL nao, SGB_EIGVEC nao*nao).  Replaces reading
+ * TwoCenterIntegral::GetValueFromArray / BaseMatrix::matrixHold_ / SCFCalculation::eigenVec. */
+int sgb_get(sgb_ctx *ctx, const sgb_mol *mol, int which, double *host, size_t count);
+
+/* ---- many molecules in one launch (batched / persistent path) -------------------------- */
+/* nmol molecules, natoms[m] atoms each; Z and xyz concatenated in molecule order. */
+int sgb_batch_create(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, const double *xyz,
+                     sgb_batch **out);
+int sgb_batch_destroy(sgb_batch *b);
+/* Replaces new coordinates for the same molecules (same atom counts and elements): one
+ * host->device copy of natoms_total*3 doubles. */
+int sgb_batch_set_coordinates(sgb_ctx *ctx, sgb_batch *b, const double *xyz);
+/* Integrals, Hcore, SCF and core-core repulsion of every molecule, one persistent launch. */
+int sgb_batch_run(sgb_ctx *ctx, sgb_batch *b, double tol, int max_iter);
+/* Per-molecule results (any pointer may be NULL).  Blocks until the run has finished. */
+int sgb_batch_results(sgb_ctx *ctx, sgb_batch *b, double *e_el, double *e_cc, int *n_iter,
+                      int *converged, int *status);
+/* One call for a set of molecules from host arrays: create (reusing the context's cached
+ * batch when the shapes match), run, read results.  e_tot may be NULL. */
+int sgb_run_molecules(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, const double *xyz,
+                      double tol, int max_iter, double *e_el, double *e_cc, int *n_iter,
+                      int *converged, int *status);
+/* Device-time of the last sgb_batch_run in milliseconds (CUDA events on the context stream). */
+int sgb_batch_last_ms(const sgb_batch *b, float *ms);
+/* Device pointer of the batch's coordinate buffer (natoms_total*3 doubles) for callers that
+ * stage inputs themselves. */
+int sgb_batch_device_coordinates(sgb_batch *b, void **dptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEMIGPU_B200_H */

@@ -1,0 +1,278 @@
+"""semigpu_b200: MNDO SCF engine for NVIDIA B200, Python access to its C ABI.
+
+The compute path is the CUDA library ``libsemigpu_b200.so`` built in-tree for sm_100a
+(``python -m semigpu_b200.build``).  This module only marshals arrays through ctypes; there is
+no CPU implementation behind it.  If the library is missing, every entry point raises.
+
+Reference interface mirrored (LuisAlfredoNu/semiGPU, src/common): the stage API of
+``src/App/semiGPU.cc:29-104`` — two-center integrals, Hcore, SCF, core-core repulsion — on one
+molecule (:class:`Molecule`), plus a batched path for many molecules (:class:`Batch`,
+:func:`run_molecules`).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import geometry
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsemigpu_b200.so")
+
+OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN = (
+    0, -1, -2, -3, -4, -5, -6, 1, 2)
+BLOCKS, HCORE, FOCK, DENSITY, EIGVAL, EIGVEC = range(6)
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_VP = ctypes.c_void_p
+
+# name -> (restype, argtypes); the exported C ABI of include/semigpu_b200.h
+SIGNATURES = {
+    "sgb_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_size_t, ctypes.POINTER(_VP)]),
+    "sgb_ctx_destroy": (ctypes.c_int, [_VP]),
+    "sgb_ctx_synchronize": (ctypes.c_int, [_VP]),
+    "sgb_last_error": (ctypes.c_char_p, [_VP]),
+    "sgb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
+    "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
+    "sgb_mol_destroy": (ctypes.c_int, [_VP]),
+    "sgb_mol_info": (ctypes.c_int, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
+    "sgb_two_center": (ctypes.c_int, [_VP, _VP]),
+    "sgb_hcore": (ctypes.c_int, [_VP, _VP]),
+    "sgb_scf": (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP, _D]),
+    "sgb_core_core": (ctypes.c_int, [_VP, _VP, _D]),
+    "sgb_fock": (ctypes.c_int, [_VP, _VP, _D, _D, _D]),
+    "sgb_get": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _D, ctypes.c_size_t]),
+    "sgb_batch_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.POINTER(_VP)]),
+    "sgb_batch_destroy": (ctypes.c_int, [_VP]),
+    "sgb_batch_set_coordinates": (ctypes.c_int, [_VP, _VP, _D]),
+    "sgb_batch_run": (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int]),
+    "sgb_batch_results": (ctypes.c_int, [_VP, _VP, _D, _D, _I, _I, _I]),
+    "sgb_run_molecules": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.c_double,
+                                         ctypes.c_int, _D, _D, _I, _I, _I]),
+    "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "sgb_batch_device_coordinates": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+}
+
+_lib = None
+
+
+class SGBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """The CUDA library; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m semigpu_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype, fn.argtypes = res, args
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+def _i(a):
+    return a.ctypes.data_as(_I)
+
+
+class _ScfResult(ctypes.Structure):
+    _fields_ = [("e_el", ctypes.c_double), ("n_iter", ctypes.c_int),
+                ("converged", ctypes.c_int), ("status", ctypes.c_int)]
+
+
+class Context:
+    """One device, one stream (sgb_ctx)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = _VP()
+        rc = lib().sgb_ctx_create(device, hbm_budget, ctypes.byref(h))
+        if rc:
+            raise SGBError(rc, f"sgb_ctx_create(device={device}) failed: "
+                               f"{lib().sgb_status_string(rc).decode()}")
+        self.h = h
+
+    def check(self, rc: int, what: str = ""):
+        if rc < 0:
+            raise SGBError(rc, f"{what}: {lib().sgb_last_error(self.h).decode()}")
+        return rc
+
+    def synchronize(self):
+        self.check(lib().sgb_ctx_synchronize(self.h), "synchronize")
+
+    @property
+    def bytes_in_use(self) -> int:
+        return int(lib().sgb_ctx_bytes_in_use(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgb_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Molecule:
+    """One molecule on the device, driven stage by stage like the reference CLI."""
+
+    def __init__(self, ctx: Context, Z, xyz):
+        self.ctx = ctx
+        self.Z = np.ascontiguousarray(Z, np.int32)
+        self.xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1)
+        h = _VP()
+        ctx.check(lib().sgb_mol_create(ctx.h, len(self.Z), _i(self.Z), _d(self.xyz),
+                                       ctypes.byref(h)), "sgb_mol_create")
+        self.h = h
+        na, nao, nocc, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        lib().sgb_mol_info(h, ctypes.byref(na), ctypes.byref(nao), ctypes.byref(nocc),
+                           ctypes.byref(nb))
+        self.natoms, self.nao, self.nocc, self.nblocks = na.value, nao.value, nocc.value, nb.value
+
+    @classmethod
+    def from_geometry(cls, ctx: Context, mol: geometry.Molecule) -> "Molecule":
+        return cls(ctx, mol.Z, mol.xyz)
+
+    def two_center(self):
+        self.ctx.check(lib().sgb_two_center(self.ctx.h, self.h), "sgb_two_center")
+
+    def hcore(self):
+        self.ctx.check(lib().sgb_hcore(self.ctx.h, self.h), "sgb_hcore")
+
+    def scf(self, tol: float = 5e-3, max_iter: int = 100) -> dict:
+        r = _ScfResult()
+        en = np.zeros(max_iter + 1)
+        rc = lib().sgb_scf(self.ctx.h, self.h, tol, max_iter, ctypes.byref(r), _d(en))
+        self.ctx.check(rc, "sgb_scf")
+        return {"E_el": r.e_el, "n_iter": r.n_iter, "converged": bool(r.converged),
+                "status": r.status, "energies": en[: r.n_iter + 1]}
+
+    def core_core(self) -> float:
+        e = ctypes.c_double()
+        self.ctx.check(lib().sgb_core_core(self.ctx.h, self.h, ctypes.byref(e)), "sgb_core_core")
+        return e.value
+
+    def fock(self, P):
+        P = np.ascontiguousarray(P, np.float64)
+        F = np.zeros(self.nao * (self.nao + 1) // 2)
+        e = ctypes.c_double()
+        self.ctx.check(lib().sgb_fock(self.ctx.h, self.h, _d(P), _d(F), ctypes.byref(e)), "sgb_fock")
+        return F, e.value
+
+    def get(self, which: int) -> np.ndarray:
+        n = self.nao
+        size = {BLOCKS: self.nblocks, HCORE: n * (n + 1) // 2, FOCK: n * (n + 1) // 2,
+                DENSITY: n * (n + 1) // 2, EIGVAL: n, EIGVEC: n * n}[which]
+        out = np.zeros(size)
+        self.ctx.check(lib().sgb_get(self.ctx.h, self.h, which, _d(out), size), "sgb_get")
+        return out
+
+    def run(self, tol: float = 5e-3, max_iter: int = 100) -> dict:
+        """All stages in the reference CLI's order (semiGPU.cc:58-95)."""
+        self.two_center()
+        self.hcore()
+        r = self.scf(tol, max_iter)
+        r["E_cc"] = self.core_core()
+        r["E_tot"] = r["E_el"] + r["E_cc"]
+        return r
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgb_mol_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _concat(mols):
+    natoms = np.array([m.natoms for m in mols], np.int32)
+    Z = np.ascontiguousarray(np.concatenate([m.Z for m in mols]), np.int32)
+    xyz = np.ascontiguousarray(np.concatenate([m.xyz.reshape(-1) for m in mols]), np.float64)
+    return natoms, Z, xyz
+
+
+class Batch:
+    """Many molecules resident on the device, run by one persistent launch."""
+
+    def __init__(self, ctx: Context, mols):
+        self.ctx = ctx
+        self.natoms, self.Z, self.xyz = _concat(mols)
+        self.nmol = len(mols)
+        h = _VP()
+        ctx.check(lib().sgb_batch_create(ctx.h, self.nmol, _i(self.natoms), _i(self.Z),
+                                         _d(self.xyz), ctypes.byref(h)), "sgb_batch_create")
+        self.h = h
+
+    def set_coordinates(self, xyz):
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1)
+        self.ctx.check(lib().sgb_batch_set_coordinates(self.ctx.h, self.h, _d(xyz)), "set_coordinates")
+
+    def run(self, tol: float = 1e-6, max_iter: int = 100):
+        self.ctx.check(lib().sgb_batch_run(self.ctx.h, self.h, tol, max_iter), "sgb_batch_run")
+
+    def results(self) -> dict:
+        n = self.nmol
+        eel, ecc = np.zeros(n), np.zeros(n)
+        it, cv, st = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+        self.ctx.check(lib().sgb_batch_results(self.ctx.h, self.h, _d(eel), _d(ecc), _i(it),
+                                               _i(cv), _i(st)), "sgb_batch_results")
+        return {"E_el": eel, "E_cc": ecc, "E_tot": eel + ecc, "n_iter": it,
+                "converged": cv.astype(bool), "status": st}
+
+    def last_ms(self) -> float:
+        ms = ctypes.c_float()
+        lib().sgb_batch_last_ms(self.h, ctypes.byref(ms))
+        return ms.value
+
+    def device_coordinates(self) -> int:
+        p = _VP()
+        lib().sgb_batch_device_coordinates(self.h, ctypes.byref(p))
+        return p.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgb_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_molecules(ctx: Context, mols, tol: float = 1e-6, max_iter: int = 100) -> dict:
+    """Host arrays in, per-molecule results out (sgb_run_molecules)."""
+    natoms, Z, xyz = _concat(mols)
+    n = len(mols)
+    eel, ecc = np.zeros(n), np.zeros(n)
+    it, cv, st = np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros(n, np.int32)
+    ctx.check(lib().sgb_run_molecules(ctx.h, n, _i(natoms), _i(Z), _d(xyz), tol, max_iter,
+                                      _d(eel), _d(ecc), _i(it), _i(cv), _i(st)), "sgb_run_molecules")
+    return {"E_el": eel, "E_cc": ecc, "E_tot": eel + ecc, "n_iter": it,
+            "converged": cv.astype(bool), "status": st}

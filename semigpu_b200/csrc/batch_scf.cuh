@@ -1,0 +1,257 @@
+// Persistent batched SCF: one CTA runs one molecule's whole calculation (integrals, Hcore,
+// guess, SCF loop, core-core repulsion) and then takes the next molecule from a work counter.
+// Molecules are handed out in the order given by `order` (the host sorts by estimated cost,
+// largest first, so the tail of the launch holds the cheap ones).
+//
+// Shared memory holds the n x n Fock/Jacobi matrix (odd leading dimension, so a column walk
+// does not hit one bank), the per-atom pair densities, the Jacobi rotation parameters and a
+// few reduction slots.  Eigenvectors, Hcore, P and F live in global memory (L2-resident at
+// these sizes).
+//
+// The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
+// repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
+// max_iter steps.  The eigensolve after the first step is warm-started: the previous
+// eigenvectors V nearly diagonalise the new F, so Jacobi runs on V^T F V with V as the initial
+// accumulated rotation, and converges in one or two sweeps.
+#pragma once
+#include "scf_block.cuh"
+
+namespace sgb {
+
+struct BatchArgs {
+  int nmol;
+  const MolDesc* mols;
+  const int* order;
+  int* counter;
+  const int8_t* slot;
+  const double* pos;
+  const int* first;
+  const int64_t* row_off;
+  const int* hb;
+  double* ints;
+  double* H;
+  double* P;
+  double* F;
+  double* V;
+  double* T;
+  double* eig;
+  double* e_el;
+  double* e_cc;
+  int* n_iter;
+  int* converged;
+  int* status;
+  double* hist;     // optional energy history, hist_stride doubles per molecule
+  int hist_stride;
+  double tol;
+  int max_iter;
+  int nmax;         // largest nao in the launch (sizes the shared memory)
+  int sorted_vectors;
+  int stages;       // STAGE_* bits
+};
+
+enum : int { STAGE_INTS = 1, STAGE_HCORE = 2, STAGE_SCF = 4, STAGE_CC = 8, STAGE_ALL = 15,
+             STAGE_FOCK = 16 /* F and E_el from the P already in device memory */ };
+
+enum : int { MOL_OK = 0, MOL_EIG_FAILED = 1, MOL_NAN = 2 };
+
+__host__ __device__ inline int smem_ld(int n) { return n | 1; }
+
+// Shared memory doubles for a launch whose largest molecule has nao = nmax.
+__host__ __device__ inline size_t batch_smem_doubles(int nmax) {
+  const size_t ld = (size_t)smem_ld(nmax);
+  const size_t ne2 = (size_t)(nmax + 2) / 2;
+  return (size_t)nmax * ld      // As
+         + 3 * (size_t)nmax + 8  // wq (<= 2.5 n) + pad
+         + 3 * ne2               // Jacobi c, s, t
+         + (size_t)nmax          // eigenvalues of the last eigensolve
+         + 32                    // reductions
+         + (size_t)nmax / 2 + 1; // occupied index list (ints, two per double)
+}
+
+__device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& d) {
+  MolView v;
+  v.natoms = d.natoms; v.nao = d.nao; v.nocc = d.nocc;
+  v.slot = a.slot + d.atom0;
+  v.pos = a.pos + 3 * d.atom0;
+  v.first = a.first + d.atom0;
+  v.row_off = a.row_off + d.atom0;
+  v.hb = a.hb + d.atom0;
+  v.ints = a.ints + d.blk0;
+  v.H = a.H + d.pk0; v.P = a.P + d.pk0; v.F = a.F + d.pk0;
+  v.V = a.V + d.sq0; v.T = a.T + d.sq0;
+  v.eig = a.eig + d.ao0;
+  return v;
+}
+
+// P (packed) = 2 Vo Vo^T with Vo = n x nocc in shared memory (ldo), 4x4 register tiles on the
+// lower triangle of tiles.
+__device__ inline void block_density(int n, int nocc, const double* Vo, int ldo, double* P) {
+  const int tiles = (n + 3) >> 2;
+  const int ntile = tiles * (tiles + 1) / 2;
+  for (int t = threadIdx.x; t < ntile; t += blockDim.x) {
+    int ti, tj;
+    {
+      int a = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+      while ((a + 1) * (a + 2) / 2 <= t) ++a;
+      while (a * (a + 1) / 2 > t) --a;
+      ti = a; tj = t - a * (a + 1) / 2;
+    }
+    const int i0 = ti * 4, j0 = tj * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    for (int k = 0; k < nocc; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) a[r] = i0 + r < n ? Vo[(i0 + r) * ldo + k] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) b[c] = j0 + c < n ? Vo[(j0 + c) * ldo + k] : 0.0;
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int i = i0 + r, j = j0 + c;
+        if (i < n && j <= i) P[tri(i) + j] = 2.0 * acc[r][c];
+      }
+  }
+}
+
+template <int NT>
+__device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
+  const MolDesc d = a.mols[mi];
+  const MolView m = make_view(a, d);
+  const int n = m.nao, ld = smem_ld(n);
+  const size_t nmax = (size_t)a.nmax;
+  double* As = smem;
+  double* wq = As + nmax * smem_ld(a.nmax);
+  double* jc = wq + 3 * nmax + 8;
+  const size_t ne2 = (nmax + 2) / 2;
+  double* js_ = jc + ne2;
+  double* jt = js_ + ne2;
+  double* dval = jt + ne2;
+  double* red = dval + nmax;
+  int* occ = reinterpret_cast<int*>(red + 32);
+  JacobiScratch js{jc, js_, jt, red};
+
+  if (a.stages & STAGE_INTS) {
+    block_integrals(m);
+    __syncthreads();
+  }
+  if (a.stages & STAGE_HCORE) {
+    block_hcore(m);
+    __syncthreads();
+  }
+  double E = 0.0;
+  int steps = 0, conv = 0, status = MOL_OK;
+  if (a.stages & STAGE_SCF) {
+    block_guess(m);
+    __syncthreads();
+    E = block_fock_energy<NT>(m, As, ld, wq, red);
+    if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
+    while (!conv && steps < a.max_iter) {
+      // ---- eigensolve of F (in As) ----
+      if (steps == 0) {
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x)
+          m.V[t] = (t / n == t % n) ? 1.0 : 0.0;
+      } else {
+        block_gemm<false>(n, As, ld, m.V, n, m.T, n);  // T = F V
+        __syncthreads();
+        block_gemm<true>(n, m.V, n, m.T, n, As, ld);   // As = V^T T
+        __syncthreads();
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+          const int i = t / n, j = t % n;
+          if (i < j) {
+            const double s = 0.5 * (As[i * ld + j] + As[j * ld + i]);
+            As[i * ld + j] = s;
+            As[j * ld + i] = s;
+          }
+        }
+      }
+      __syncthreads();
+      const int sw = block_jacobi<NT>(n, As, ld, m.V, js, 1e-14, 60);
+      if (sw < 0) { status = MOL_EIG_FAILED; break; }
+      // ---- eigenvalues, occupied set ----
+      for (int i = threadIdx.x; i < n; i += blockDim.x) dval[i] = As[i * ld + i];
+      __syncthreads();
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double di = dval[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+          const double dj = dval[j];
+          rank += (dj < di) || (dj == di && j < i);
+        }
+        if (rank < m.nocc) occ[rank] = i;
+      }
+      __syncthreads();
+      // ---- density from the occupied vectors (gathered into shared memory) ----
+      const int ldo = m.nocc | 1;
+      for (int t = threadIdx.x; t < n * m.nocc; t += blockDim.x) {
+        const int i = t / m.nocc, k = t % m.nocc;
+        As[i * ldo + k] = m.V[(int64_t)i * n + occ[k]];
+      }
+      __syncthreads();
+      block_density(n, m.nocc, As, ldo, m.P);
+      __syncthreads();
+      // ---- Fock + energy ----
+      const double Eold = E;
+      E = block_fock_energy<NT>(m, As, ld, wq, red);
+      ++steps;
+      if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride + steps] = E;
+      if (E != E) { status = MOL_NAN; break; }
+      conv = fabs(Eold - E) < a.tol;
+    }
+    // eigenvalues (ascending) and, on request, eigenvectors sorted the same way into T
+    if (steps > 0) {
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double di = dval[i];
+        int rank = 0;
+        for (int j = 0; j < n; ++j) {
+          const double dj = dval[j];
+          rank += (dj < di) || (dj == di && j < i);
+        }
+        m.eig[rank] = di;
+        if (a.sorted_vectors)
+          for (int r = 0; r < n; ++r) m.T[(int64_t)r * n + rank] = m.V[(int64_t)r * n + i];
+      }
+    }
+  }
+  if (a.stages & STAGE_FOCK) {
+    E = block_fock_energy<NT>(m, nullptr, 0, wq, red);
+    if (threadIdx.x == 0) a.e_el[mi] = E;
+  }
+  double ecc = 0.0;
+  if (a.stages & STAGE_CC) ecc = block_core_core<NT>(m, red);
+  if (threadIdx.x == 0) {
+    if (a.stages & STAGE_SCF) {
+      a.e_el[mi] = E;
+      a.n_iter[mi] = steps;
+      a.converged[mi] = conv;
+      a.status[mi] = status;
+    }
+    if (a.stages & STAGE_CC) a.e_cc[mi] = ecc;
+  }
+  __syncthreads();
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
+  extern __shared__ double smem[];
+  __shared__ int s_next;
+  for (;;) {
+    if (threadIdx.x == 0) s_next = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int q = s_next;
+    __syncthreads();
+    if (q >= a.nmol) break;
+    run_molecule<NT>(a, a.order[q], smem);
+  }
+}
+
+}  // namespace sgb

@@ -1,0 +1,577 @@
+// C ABI of the engine (include/semigpu_b200.h).  One translation unit: the device tables live
+// in this TU's constant bank, and every kernel is instantiated here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/semigpu_b200.h"
+#include "batch_scf.cuh"
+#include "layout.h"
+#include "mndo_tables.cuh"
+
+using namespace sgb;
+
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kSmallNmax = 160;  // largest nao whose n x n FP64 matrix fits one CTA's smem
+constexpr size_t kAlign = 256;
+
+__global__ void k_ang_to_bohr(const double* __restrict__ xyz, double* __restrict__ pos,
+                              int64_t count) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x)
+    pos[i] = xyz[i] * kAng2Bohr;
+}
+
+}  // namespace
+
+struct sgb_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0;
+  size_t in_use = 0;
+  int num_sms = 0;
+  size_t smem_optin = 0;
+  std::string err;
+  sgb_batch* cached = nullptr;  // reused by sgb_run_molecules
+};
+
+struct sgb_batch {
+  sgb_ctx* ctx = nullptr;
+  int nmol = 0;
+  int64_t natoms_total = 0;
+  int nmax = 0;
+  std::vector<MolDesc> desc;
+  std::vector<int> order;
+  std::vector<int> natoms;
+  std::vector<int> Z;
+  char* arena = nullptr;
+  size_t bytes = 0;
+  MolDesc* d_desc = nullptr;
+  int* d_order = nullptr;
+  int* d_counter = nullptr;
+  int8_t* d_slot = nullptr;
+  double* d_xyz = nullptr;
+  double* d_pos = nullptr;
+  int* d_first = nullptr;
+  int64_t* d_row_off = nullptr;
+  int* d_hb = nullptr;
+  double *d_ints = nullptr, *d_H = nullptr, *d_P = nullptr, *d_F = nullptr;
+  double *d_V = nullptr, *d_T = nullptr, *d_eig = nullptr;
+  double *d_eel = nullptr, *d_ecc = nullptr;
+  int *d_niter = nullptr, *d_conv = nullptr, *d_status = nullptr;
+  double* d_hist = nullptr;
+  int hist_stride = 0;
+  int64_t n_ints = 0, n_pk = 0, n_sq = 0, n_ao = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  float last_ms = 0.f;
+};
+
+struct sgb_mol {
+  sgb_ctx* ctx = nullptr;
+  sgb_batch* b = nullptr;
+  bool ints_done = false, hcore_done = false, scf_done = false;
+};
+
+namespace {
+
+int fail(sgb_ctx* ctx, int code, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return code;
+}
+
+int cuda_fail(sgb_ctx* ctx, cudaError_t e, const char* what) {
+  return fail(ctx, SGB_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CUDA_TRY(ctx, call)                                  \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// Estimated SCF cost used to order the persistent launch (largest first).
+double cost_of(const MolDesc& d) { return (double)d.nao * d.nao * d.nao + 50.0 * d.natoms * d.natoms; }
+
+void free_batch(sgb_batch* b) {
+  if (!b) return;
+  if (b->arena) {
+    cudaFree(b->arena);
+    if (b->ctx) b->ctx->in_use -= b->bytes;
+  }
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+}
+
+int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const double* xyz,
+                int hist_stride, sgb_batch** out) {
+  if (!ctx || !out || nmol <= 0 || !natoms || !Z || !xyz)
+    return fail(ctx, SGB_E_ARG, "batch: null pointer or nmol <= 0");
+  auto* b = new sgb_batch();
+  b->ctx = ctx;
+  b->nmol = nmol;
+  b->desc.resize(nmol);
+  b->natoms.assign(natoms, natoms + nmol);
+  int64_t atom0 = 0, blk0 = 0, pk0 = 0, sq0 = 0, ao0 = 0;
+  std::vector<int8_t> slot;
+  std::vector<int> first, hb;
+  std::vector<int64_t> row_off;
+  for (int m = 0; m < nmol; ++m) {
+    const int na = natoms[m];
+    if (na <= 0) { delete b; return fail(ctx, SGB_E_ARG, "molecule %d has %d atoms", m, na); }
+    MolDesc& d = b->desc[m];
+    d.natoms = na;
+    d.atom0 = atom0;
+    int nao = 0, nel = 0, nheavy = 0;
+    int64_t roff = 0;
+    for (int a = 0; a < na; ++a) {
+      const int z = Z[atom0 + a];
+      const int s = slot_of(z);
+      if (s < 0) {
+        delete b;
+        return fail(ctx, SGB_E_ELEMENT,
+                    "molecule %d atom %d: Z=%d has no MNDO parameters (supported: H C N O)", m, a, z);
+      }
+      slot.push_back((int8_t)s);
+      first.push_back(nao);
+      hb.push_back(nheavy);
+      row_off.push_back(roff);
+      // row size of atom a (blocks against atoms 0..a)
+      const bool heavy = s != 0;
+      const int nh = nheavy + (heavy ? 1 : 0), nl = a + 1 - nh;
+      roff += (int64_t)nh * (heavy ? 100 : 10) + (int64_t)nl * (heavy ? 10 : 1);
+      nao += heavy ? 4 : 1;
+      nel += s == 0 ? 1 : (z - 2);
+      nheavy += heavy ? 1 : 0;
+      b->Z.push_back(z);
+    }
+    d.nao = nao;
+    d.nocc = nel / 2;
+    d.nheavy = nheavy;
+    d.nblk = roff;
+    d.blk0 = blk0;
+    d.pk0 = pk0;
+    d.sq0 = sq0;
+    d.ao0 = ao0;
+    blk0 += (roff + 31) / 32 * 32;
+    pk0 += (tri(nao) + 31) / 32 * 32;
+    sq0 += ((int64_t)nao * nao + 31) / 32 * 32;
+    ao0 += (nao + 31) / 32 * 32;
+    atom0 += na;
+    b->nmax = std::max(b->nmax, nao);
+  }
+  b->natoms_total = atom0;
+  b->n_ints = blk0; b->n_pk = pk0; b->n_sq = sq0; b->n_ao = ao0;
+  b->hist_stride = hist_stride;
+  b->order.resize(nmol);
+  for (int m = 0; m < nmol; ++m) b->order[m] = m;
+  std::stable_sort(b->order.begin(), b->order.end(),
+                   [&](int x, int y) { return cost_of(b->desc[x]) > cost_of(b->desc[y]); });
+
+  // one arena
+  const int64_t NA = atom0;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
+  const size_t o_desc = take(sizeof(MolDesc) * nmol), o_order = take(sizeof(int) * nmol),
+               o_counter = take(sizeof(int)), o_slot = take(NA), o_xyz = take(24 * NA),
+               o_pos = take(24 * NA), o_first = take(4 * NA), o_roff = take(8 * NA),
+               o_hb = take(4 * NA), o_ints = take(8 * b->n_ints), o_H = take(8 * b->n_pk),
+               o_P = take(8 * b->n_pk), o_F = take(8 * b->n_pk), o_V = take(8 * b->n_sq),
+               o_T = take(8 * b->n_sq), o_eig = take(8 * b->n_ao), o_eel = take(8 * nmol),
+               o_ecc = take(8 * nmol), o_nit = take(4 * nmol), o_conv = take(4 * nmol),
+               o_stat = take(4 * nmol),
+               o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0);
+  b->bytes = off;
+  if (ctx->budget && ctx->in_use + off > ctx->budget) {
+    delete b;
+    return fail(ctx, SGB_E_NOMEM, "batch needs %zu bytes; budget %zu, in use %zu", off,
+                ctx->budget, ctx->in_use);
+  }
+  cudaError_t e = cudaMalloc(&b->arena, off);
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
+  }
+  ctx->in_use += off;
+  char* base = b->arena;
+  b->d_desc = (MolDesc*)(base + o_desc);
+  b->d_order = (int*)(base + o_order);
+  b->d_counter = (int*)(base + o_counter);
+  b->d_slot = (int8_t*)(base + o_slot);
+  b->d_xyz = (double*)(base + o_xyz);
+  b->d_pos = (double*)(base + o_pos);
+  b->d_first = (int*)(base + o_first);
+  b->d_row_off = (int64_t*)(base + o_roff);
+  b->d_hb = (int*)(base + o_hb);
+  b->d_ints = (double*)(base + o_ints);
+  b->d_H = (double*)(base + o_H);
+  b->d_P = (double*)(base + o_P);
+  b->d_F = (double*)(base + o_F);
+  b->d_V = (double*)(base + o_V);
+  b->d_T = (double*)(base + o_T);
+  b->d_eig = (double*)(base + o_eig);
+  b->d_eel = (double*)(base + o_eel);
+  b->d_ecc = (double*)(base + o_ecc);
+  b->d_niter = (int*)(base + o_nit);
+  b->d_conv = (int*)(base + o_conv);
+  b->d_status = (int*)(base + o_stat);
+  b->d_hist = hist_stride > 0 ? (double*)(base + o_hist) : nullptr;
+  cudaStream_t st = ctx->stream;
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
+  };
+  if ((e = up(b->d_desc, b->desc.data(), sizeof(MolDesc) * nmol)) != cudaSuccess ||
+      (e = up(b->d_order, b->order.data(), sizeof(int) * nmol)) != cudaSuccess ||
+      (e = up(b->d_slot, slot.data(), NA)) != cudaSuccess ||
+      (e = up(b->d_xyz, xyz, 24 * NA)) != cudaSuccess ||
+      (e = up(b->d_first, first.data(), 4 * NA)) != cudaSuccess ||
+      (e = up(b->d_row_off, row_off.data(), 8 * NA)) != cudaSuccess ||
+      (e = up(b->d_hb, hb.data(), 4 * NA)) != cudaSuccess ||
+      (e = cudaMemsetAsync(b->d_status, 0, 4 * nmol, st)) != cudaSuccess ||
+      (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
+    free_batch(b);
+    return cuda_fail(ctx, e, "batch upload");
+  }
+  k_ang_to_bohr<<<std::max<int64_t>(1, std::min<int64_t>((3 * NA + 255) / 256, 1024)), 256, 0, st>>>(
+      b->d_xyz, b->d_pos, 3 * NA);
+  if ((e = cudaGetLastError()) != cudaSuccess) {
+    free_batch(b);
+    return cuda_fail(ctx, e, "k_ang_to_bohr");
+  }
+  *out = b;
+  return SGB_OK;
+}
+
+int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_iter,
+                  int sorted_vectors) {
+  const bool needs_smem = stages & (STAGE_SCF | STAGE_FOCK);
+  if (needs_smem && b->nmax > kSmallNmax)
+    return fail(ctx, SGB_E_UNSUPPORTED,
+                "SCF/Fock for nao=%d: the in-shared-memory path takes nao <= %d", b->nmax, kSmallNmax);
+  BatchArgs a;
+  a.nmol = b->nmol;
+  a.mols = b->d_desc;
+  a.order = b->d_order;
+  a.counter = b->d_counter;
+  a.slot = b->d_slot;
+  a.pos = b->d_pos;
+  a.first = b->d_first;
+  a.row_off = b->d_row_off;
+  a.hb = b->d_hb;
+  a.ints = b->d_ints;
+  a.H = b->d_H; a.P = b->d_P; a.F = b->d_F;
+  a.V = b->d_V; a.T = b->d_T; a.eig = b->d_eig;
+  a.e_el = b->d_eel; a.e_cc = b->d_ecc;
+  a.n_iter = b->d_niter; a.converged = b->d_conv; a.status = b->d_status;
+  a.hist = b->d_hist; a.hist_stride = b->hist_stride;
+  a.tol = tol;
+  a.max_iter = std::min(max_iter, b->hist_stride > 0 ? b->hist_stride - 1 : max_iter);
+  a.nmax = std::max(1, std::min(b->nmax, kSmallNmax));
+  a.sorted_vectors = sorted_vectors;
+  a.stages = stages;
+  const size_t smem = needs_smem ? batch_smem_doubles(a.nmax) * sizeof(double) : 0;
+  cudaStream_t st = ctx->stream;
+  CUDA_TRY(ctx, cudaFuncSetAttribute(k_batch_scf<kThreads>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_scf<kThreads>,
+                                                              kThreads, smem));
+  if (per_sm < 1) return fail(ctx, SGB_E_CUDA, "kernel does not fit an SM (smem %zu)", smem);
+  const int grid = std::min(b->nmol, per_sm * ctx->num_sms);
+  CUDA_TRY(ctx, cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+  CUDA_TRY(ctx, cudaEventRecord(b->ev0, st));
+  k_batch_scf<kThreads><<<grid, kThreads, smem, st>>>(a);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaEventRecord(b->ev1, st));
+  return SGB_OK;
+}
+
+}  // namespace
+
+// ============================================================================================
+extern "C" {
+
+const char* sgb_status_string(int s) {
+  switch (s) {
+    case SGB_OK: return "ok";
+    case SGB_E_ARG: return "invalid argument";
+    case SGB_E_ELEMENT: return "element without MNDO parameters";
+    case SGB_E_CUDA: return "CUDA error";
+    case SGB_E_NOMEM: return "out of device memory or over budget";
+    case SGB_E_STATE: return "stage called out of order";
+    case SGB_E_UNSUPPORTED: return "unsupported size";
+    case SGB_E_EIG: return "eigensolver did not converge";
+    case SGB_E_NAN: return "non-finite energy";
+    default: return "unknown status";
+  }
+}
+
+const char* sgb_last_error(const sgb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+size_t sgb_ctx_bytes_in_use(const sgb_ctx* ctx) { return ctx ? ctx->in_use : 0; }
+
+int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
+  if (!out) return SGB_E_ARG;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || device < 0 || device >= n) return SGB_E_CUDA;
+  auto* c = new sgb_ctx();
+  c->device = device;
+  c->budget = budget;
+  if ((e = cudaSetDevice(device)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = upload_tables()) != cudaSuccess ||
+      (e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
+    delete c;
+    return SGB_E_CUDA;
+  }
+  int optin = 0;
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  c->smem_optin = optin;
+  *out = c;
+  return SGB_OK;
+}
+
+int sgb_ctx_destroy(sgb_ctx* ctx) {
+  if (!ctx) return SGB_E_ARG;
+  cudaSetDevice(ctx->device);
+  free_batch(ctx->cached);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return SGB_OK;
+}
+
+int sgb_ctx_synchronize(sgb_ctx* ctx) {
+  if (!ctx) return SGB_E_ARG;
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return SGB_OK;
+}
+
+// ---- one molecule ---------------------------------------------------------------------------
+int sgb_mol_create(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, sgb_mol** out) {
+  if (!ctx || !out) return SGB_E_ARG;
+  *out = nullptr;
+  sgb_batch* b = nullptr;
+  int rc = build_batch(ctx, 1, &natoms, Z, xyz, 101, &b);
+  if (rc) return rc;
+  auto* m = new sgb_mol();
+  m->ctx = ctx;
+  m->b = b;
+  *out = m;
+  return SGB_OK;
+}
+
+int sgb_mol_destroy(sgb_mol* mol) {
+  if (!mol) return SGB_E_ARG;
+  free_batch(mol->b);
+  delete mol;
+  return SGB_OK;
+}
+
+int sgb_mol_info(const sgb_mol* mol, int* natoms, int* nao, int* nocc, long long* nblocks) {
+  if (!mol) return SGB_E_ARG;
+  const MolDesc& d = mol->b->desc[0];
+  if (natoms) *natoms = d.natoms;
+  if (nao) *nao = d.nao;
+  if (nocc) *nocc = d.nocc;
+  if (nblocks) *nblocks = d.nblk;
+  return SGB_OK;
+}
+
+int sgb_two_center(sgb_ctx* ctx, sgb_mol* mol) {
+  if (!ctx || !mol) return SGB_E_ARG;
+  int rc = launch_stages(ctx, mol->b, STAGE_INTS, 0.0, 0, 0);
+  if (rc) return rc;
+  mol->ints_done = true;
+  mol->hcore_done = mol->scf_done = false;
+  return sgb_ctx_synchronize(ctx);
+}
+
+int sgb_hcore(sgb_ctx* ctx, sgb_mol* mol) {
+  if (!ctx || !mol) return SGB_E_ARG;
+  if (!mol->ints_done) return fail(ctx, SGB_E_STATE, "Hcore needs the two-center integrals");
+  int rc = launch_stages(ctx, mol->b, STAGE_HCORE, 0.0, 0, 0);
+  if (rc) return rc;
+  mol->hcore_done = true;
+  return sgb_ctx_synchronize(ctx);
+}
+
+int sgb_scf(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result* res,
+            double* energies) {
+  if (!ctx || !mol || max_iter < 0 || !(tol >= 0.0)) return SGB_E_ARG;
+  if (!mol->hcore_done) return fail(ctx, SGB_E_STATE, "SCF needs Hcore");
+  if (max_iter > mol->b->hist_stride - 1)
+    return fail(ctx, SGB_E_ARG, "max_iter %d above %d", max_iter, mol->b->hist_stride - 1);
+  int rc = launch_stages(ctx, mol->b, STAGE_SCF, tol, max_iter, 1);
+  if (rc) return rc;
+  sgb_batch* b = mol->b;
+  double e_el = 0.0;
+  int it = 0, cv = 0, st = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&e_el, b->d_eel, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(&it, b->d_niter, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(&cv, b->d_conv, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaMemcpyAsync(&st, b->d_status, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (energies)
+    CUDA_TRY(ctx, cudaMemcpy(energies, b->d_hist, 8 * (size_t)(it + 1), cudaMemcpyDeviceToHost));
+  if (res) {
+    res->e_el = e_el;
+    res->n_iter = it;
+    res->converged = cv;
+    res->status = st == MOL_OK ? SGB_OK : st == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN;
+  }
+  mol->scf_done = true;
+  return st == MOL_OK ? SGB_OK : st == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN;
+}
+
+int sgb_core_core(sgb_ctx* ctx, sgb_mol* mol, double* e_cc) {
+  if (!ctx || !mol || !e_cc) return SGB_E_ARG;
+  if (!mol->ints_done) return fail(ctx, SGB_E_STATE, "core-core needs the two-center integrals");
+  int rc = launch_stages(ctx, mol->b, STAGE_CC, 0.0, 0, 0);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaMemcpyAsync(e_cc, mol->b->d_ecc, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  return sgb_ctx_synchronize(ctx);
+}
+
+int sgb_fock(sgb_ctx* ctx, sgb_mol* mol, const double* P, double* F, double* e_el) {
+  if (!ctx || !mol || !P) return SGB_E_ARG;
+  if (!mol->hcore_done) return fail(ctx, SGB_E_STATE, "Fock needs Hcore");
+  sgb_batch* b = mol->b;
+  const size_t np = (size_t)tri(b->desc[0].nao);
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->d_P, P, 8 * np, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = launch_stages(ctx, b, STAGE_FOCK, 0.0, 0, 0);
+  if (rc) return rc;
+  if (F) CUDA_TRY(ctx, cudaMemcpyAsync(F, b->d_F, 8 * np, cudaMemcpyDeviceToHost, ctx->stream));
+  if (e_el) CUDA_TRY(ctx, cudaMemcpyAsync(e_el, b->d_eel, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  return sgb_ctx_synchronize(ctx);
+}
+
+int sgb_get(sgb_ctx* ctx, const sgb_mol* mol, int which, double* host, size_t count) {
+  if (!ctx || !mol || !host) return SGB_E_ARG;
+  const sgb_batch* b = mol->b;
+  const MolDesc& d = b->desc[0];
+  const double* src = nullptr;
+  size_t need = 0;
+  switch (which) {
+    case SGB_BLOCKS: src = b->d_ints; need = d.nblk; break;
+    case SGB_HCORE: src = b->d_H; need = tri(d.nao); break;
+    case SGB_FOCK: src = b->d_F; need = tri(d.nao); break;
+    case SGB_DENSITY: src = b->d_P; need = tri(d.nao); break;
+    case SGB_EIGVAL: src = b->d_eig; need = d.nao; break;
+    case SGB_EIGVEC: src = b->d_T; need = (size_t)d.nao * d.nao; break;
+    default: return fail(ctx, SGB_E_ARG, "unknown matrix id %d", which);
+  }
+  if (count < need) return fail(ctx, SGB_E_ARG, "buffer holds %zu, need %zu", count, need);
+  if (which == SGB_EIGVEC) {
+    // device T is row-major sorted vectors (T[r*n + k]); the reference's eigenVec is
+    // column-major, i.e. the transpose in row-major terms
+    std::vector<double> tmp(need);
+    CUDA_TRY(ctx, cudaMemcpyAsync(tmp.data(), src, 8 * need, cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    const int n = d.nao;
+    for (int r = 0; r < n; ++r)
+      for (int k = 0; k < n; ++k) host[(size_t)k * n + r] = tmp[(size_t)r * n + k];
+    return SGB_OK;
+  }
+  CUDA_TRY(ctx, cudaMemcpyAsync(host, src, 8 * need, cudaMemcpyDeviceToHost, ctx->stream));
+  return sgb_ctx_synchronize(ctx);
+}
+
+// ---- batches ---------------------------------------------------------------------------------
+int sgb_batch_create(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const double* xyz,
+                     sgb_batch** out) {
+  if (!ctx || !out) return SGB_E_ARG;
+  *out = nullptr;
+  return build_batch(ctx, nmol, natoms, Z, xyz, 0, out);
+}
+
+int sgb_batch_destroy(sgb_batch* b) {
+  if (!b) return SGB_E_ARG;
+  if (b->ctx && b->ctx->cached == b) b->ctx->cached = nullptr;
+  free_batch(b);
+  return SGB_OK;
+}
+
+int sgb_batch_set_coordinates(sgb_ctx* ctx, sgb_batch* b, const double* xyz) {
+  if (!ctx || !b || !xyz) return SGB_E_ARG;
+  const int64_t NA = b->natoms_total;
+  CUDA_TRY(ctx, cudaMemcpyAsync(b->d_xyz, xyz, 24 * NA, cudaMemcpyHostToDevice, ctx->stream));
+  k_ang_to_bohr<<<std::max<int64_t>(1, std::min<int64_t>((3 * NA + 255) / 256, 1024)), 256, 0,
+                  ctx->stream>>>(b->d_xyz, b->d_pos, 3 * NA);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return SGB_OK;
+}
+
+int sgb_batch_run(sgb_ctx* ctx, sgb_batch* b, double tol, int max_iter) {
+  if (!ctx || !b || max_iter < 0 || !(tol >= 0.0)) return SGB_E_ARG;
+  return launch_stages(ctx, b, STAGE_ALL, tol, max_iter, 0);
+}
+
+int sgb_batch_results(sgb_ctx* ctx, sgb_batch* b, double* e_el, double* e_cc, int* n_iter,
+                      int* converged, int* status) {
+  if (!ctx || !b) return SGB_E_ARG;
+  cudaStream_t st = ctx->stream;
+  const int n = b->nmol;
+  if (e_el) CUDA_TRY(ctx, cudaMemcpyAsync(e_el, b->d_eel, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  if (e_cc) CUDA_TRY(ctx, cudaMemcpyAsync(e_cc, b->d_ecc, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  if (n_iter) CUDA_TRY(ctx, cudaMemcpyAsync(n_iter, b->d_niter, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  if (converged) CUDA_TRY(ctx, cudaMemcpyAsync(converged, b->d_conv, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  if (status) CUDA_TRY(ctx, cudaMemcpyAsync(status, b->d_status, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  CUDA_TRY(ctx, cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
+  return SGB_OK;
+}
+
+int sgb_batch_last_ms(const sgb_batch* b, float* ms) {
+  if (!b || !ms) return SGB_E_ARG;
+  *ms = b->last_ms;
+  return SGB_OK;
+}
+
+int sgb_batch_device_coordinates(sgb_batch* b, void** dptr) {
+  if (!b || !dptr) return SGB_E_ARG;
+  *dptr = b->d_xyz;
+  return SGB_OK;
+}
+
+int sgb_run_molecules(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const double* xyz,
+                      double tol, int max_iter, double* e_el, double* e_cc, int* n_iter,
+                      int* converged, int* status) {
+  if (!ctx || nmol <= 0 || !natoms || !Z || !xyz) return SGB_E_ARG;
+  sgb_batch* b = ctx->cached;
+  bool same = b && b->nmol == nmol && std::equal(natoms, natoms + nmol, b->natoms.begin());
+  if (same) same = std::equal(b->Z.begin(), b->Z.end(), Z);
+  int rc;
+  if (same) {
+    rc = sgb_batch_set_coordinates(ctx, b, xyz);
+  } else {
+    free_batch(ctx->cached);
+    ctx->cached = nullptr;
+    rc = build_batch(ctx, nmol, natoms, Z, xyz, 0, &b);
+    if (!rc) ctx->cached = b;
+  }
+  if (rc) return rc;
+  rc = sgb_batch_run(ctx, b, tol, max_iter);
+  if (rc) return rc;
+  return sgb_batch_results(ctx, b, e_el, e_cc, n_iter, converged, status);
+}
+
+}  // extern "C"

@@ -1,0 +1,469 @@
+// CTA-cooperative stages of one molecule's MNDO calculation.  Every function here is called by
+// all threads of one thread block and works on one molecule (a MolView); the persistent batch
+// kernel strings them together so a molecule's whole SCF runs inside one CTA with its Fock /
+// Jacobi matrix resident in shared memory.
+//
+// Reference stages (LuisAlfredoNu/semiGPU, src/common):
+//   integrals  ComputeAllTwoCenterIntegral      twocenterintegral.cpp:229-279
+//   Hcore      Hcore::ComputeElementMatrix      hcore.cpp:25-100
+//   guess      DensityMatrix guess              densitymatrix.cpp:26-37
+//   Fock       FockMatrix / ComputeGMatrix_UV   fockmatrix.cpp:20-53, twoelectronmatrix.cpp:14-35
+//   energy     ElectronicEnergy::ComputeEnergy  electronicenergy.cpp:12-36
+//   eigensolve GetEigenValVecOfFmatrix (dsyev)  scfcalculation.cpp:171-203
+//   density    DensityMatrix::ComputeElementMatrix densitymatrix.cpp:38-46
+//   core-core  CoreCoreRepulsion                corecorerepulsion.cpp:12-65
+//
+// The Fock build uses the NDDO sparsity of the reference's own sum: (mu nu|lam sig) is zero
+// unless mu, nu share an atom and lam, sig share an atom (GetValueFromArray,
+// twocenterintegral.cpp:285-386), so F = H + G(P) reduces to a Coulomb sum per atom over all
+// atoms, a one-center exchange per atom and a two-center exchange per atom pair.
+#pragma once
+#include "layout.h"
+#include "mndo_device.cuh"
+
+namespace sgb {
+
+struct MolView {
+  int natoms, nao, nocc;
+  const int8_t* slot;      // per atom
+  const double* pos;       // 3 per atom, bohr
+  const int* first;        // first AO of each atom
+  const int64_t* row_off;  // integral block-row offsets
+  const int* hb;           // heavy atoms before each atom
+  double* ints;            // integral blocks
+  double* H;               // packed
+  double* P;               // packed
+  double* F;               // packed
+  double* V;               // n*n, row-major: V[i*n + k] = AO i of vector k
+  double* T;               // n*n scratch
+  double* eig;             // n
+};
+
+__device__ __forceinline__ int nao_of_slot(int s) { return s ? 4 : 1; }
+
+__device__ __forceinline__ const double* blk_ptr(const MolView& m, int A, int B) {
+  return m.ints + block_offset(m.row_off, m.hb, m.slot, A, B);
+}
+
+// atom pair index p -> (A, B) with A >= B, p = A(A+1)/2 + B
+__device__ __forceinline__ void tri_inverse(int64_t p, int& A, int& B) {
+  int a = (int)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
+  while (tri(a + 1) <= p) ++a;
+  while (tri(a) > p) --a;
+  A = a;
+  B = (int)(p - tri(a));
+}
+
+// Block-wide sum (all threads call; result valid in every thread).
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? red[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (l == 0) red[0] = v;
+  }
+  __syncthreads();
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------------------------------------------
+// Integrals: one thread per atom pair (A >= B), writing the pair's block.
+__device__ inline void write_pair_block(const MolView& m, int A, int B) {
+  double* blk = m.ints + block_offset(m.row_off, m.hb, m.slot, A, B);
+  const int sA = m.slot[A], sB = m.slot[B];
+  if (A == B) {
+    if (sA == 0) {
+      blk[0] = c_elem[0].gss;
+    } else {
+      for (int i = 0; i < 10; ++i)
+        for (int j = 0; j < 10; ++j)
+          blk[10 * i + j] = one_center_value(sA, pair_first(i), pair_second(i), pair_first(j),
+                                             pair_second(j));
+    }
+    return;
+  }
+  PairFrame f;
+  if (sA != 0 && sB != 0) {
+    pair_frame(sA, sB, m.pos + 3 * A, m.pos + 3 * B, f);
+    for (int i = 0; i < 10; ++i) {
+      const int a = pair_first(i), b = pair_second(i);
+      for (int j = 0; j < 10; ++j)
+        blk[10 * i + j] = two_center_value(f, a, b, pair_first(j), pair_second(j));
+    }
+  } else if (sA == 0 && sB == 0) {
+    pair_frame(0, 0, m.pos + 3 * A, m.pos + 3 * B, f);
+    blk[0] = f.v[L_SSSS] * kHartree2eV;
+  } else {
+    // H-X and X-H blocks hold (s_H s_H | pair on X), computed with the H atom first
+    // (ComputePair_HX / ComputePair_XH, twocenterintegral.cpp:400-447).
+    const int Hh = sA == 0 ? A : B, X = sA == 0 ? B : A;
+    pair_frame(0, m.slot[X], m.pos + 3 * Hh, m.pos + 3 * X, f);
+    for (int k = 0; k < 10; ++k) blk[k] = two_center_value(f, 0, 0, pair_first(k), pair_second(k));
+  }
+}
+
+__device__ inline void block_integrals(const MolView& m) {
+  const int64_t np = tri(m.natoms);
+  for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
+    int A, B;
+    tri_inverse(p, A, B);
+    write_pair_block(m, A, B);
+  }
+}
+
+// (mu nu | s_C s_C) for mu, nu on atom A (pair index pq of A), C != A.
+__device__ __forceinline__ double coulomb_ss(const MolView& m, int A, int pq, int C) {
+  const int sA = m.slot[A], sC = m.slot[C];
+  if (sA == 0) return *blk_ptr(m, A > C ? A : C, A > C ? C : A);   // (sA sA|sC sC): entry 0
+  if (sC == 0) return blk_ptr(m, A > C ? A : C, A > C ? C : A)[pq];  // H-X block, column pq
+  return A > C ? blk_ptr(m, A, C)[10 * pq] : blk_ptr(m, C, A)[pq];
+}
+
+// Hcore: off-diagonal atom blocks 1/2 (beta_mu + beta_nu) S_mu_nu (hcore.cpp:38-69), diagonal
+// atom blocks U delta + sum_{C != A} -Z_C (mu nu|s_C s_C) (hcore.cpp:71-92).
+__device__ inline void hcore_offdiag_pair(const MolView& m, int A, int B) {
+  const int sA = m.slot[A], sB = m.slot[B];
+  double S[16];
+  overlap_block(sA, sB, m.pos + 3 * A, m.pos + 3 * B, S);
+  const int nA = nao_of_slot(sA), nB = nao_of_slot(sB), fA = m.first[A], fB = m.first[B];
+  for (int mu = 0; mu < nA; ++mu) {
+    const double ba = mu ? c_elem[sA].beta_p : c_elem[sA].beta_s;
+    for (int nu = 0; nu < nB; ++nu) {
+      const double bb = nu ? c_elem[sB].beta_p : c_elem[sB].beta_s;
+      m.H[tri(fA + mu) + fB + nu] = (ba + bb) * S[4 * mu + nu] * 0.5;
+    }
+  }
+}
+
+__device__ inline void hcore_diag_atom(const MolView& m, int A, int pq) {
+  const int sA = m.slot[A];
+  double s = 0.0;
+  for (int C = 0; C < m.natoms; ++C)
+    if (C != A) s += -(double)c_elem[m.slot[C]].core * coulomb_ss(m, A, pq, C);
+  const int a = pair_first(pq), b = pair_second(pq), f = m.first[A];
+  if (a == b) s += a == 0 ? c_elem[sA].uss : c_elem[sA].upp;
+  m.H[tri(f + b) + f + a] = s;
+}
+
+__device__ inline void block_hcore(const MolView& m) {
+  const int64_t np = tri(m.natoms);
+  // diagonal blocks first: one task per (atom, pair index)
+  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) {
+    const int A = t / 10, pq = t % 10;
+    if (m.slot[A] == 0 && pq) continue;
+    hcore_diag_atom(m, A, pq);
+  }
+  for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
+    int A, B;
+    tri_inverse(p, A, B);
+    if (A != B) hcore_offdiag_pair(m, A, B);
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Fock build + electronic energy.  Writes F packed to global memory and, when Fs != nullptr,
+// the full symmetric F into shared memory (leading dimension ld).  Returns E_el in every thread.
+//
+// wq: shared scratch of 10 * nheavy + nlight doubles: the pair densities of each atom,
+//     w_C[q] = P_{lam sig} (x2 when lam != sig) for pair q = (lam, sig) of atom C.
+__device__ __forceinline__ int wq_offset(const MolView& m, int A) { return 9 * m.hb[A] + A; }
+
+template <int NT>
+__device__ double block_fock_energy(const MolView& m, double* Fs, int ld, double* wq,
+                                    double* red) {
+  // pair densities
+  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) {
+    const int C = t / 10, q = t % 10;
+    const int s = m.slot[C];
+    if (s == 0 && q) continue;
+    const int a = pair_first(q), b = pair_second(q), f = m.first[C];
+    const double p = m.P[tri(f + b) + f + a];
+    wq[wq_offset(m, C) + q] = a == b ? p : 2.0 * p;
+  }
+  __syncthreads();
+  double e = 0.0;
+  // diagonal atom blocks: task (A, pq)
+  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) {
+    const int A = t / 10, pq = t % 10;
+    const int sA = m.slot[A];
+    if (sA == 0 && pq) continue;
+    const int a = pair_first(pq), b = pair_second(pq), fA = m.first[A];
+    double J = 0.0;
+    for (int C = 0; C < m.natoms; ++C) {
+      const int sC = m.slot[C];
+      const double* w = wq + wq_offset(m, C);
+      if (sA == 0) {
+        if (sC == 0) {
+          J += *blk_ptr(m, A > C ? A : C, A > C ? C : A) * w[0];
+        } else {
+          const double* I = blk_ptr(m, A > C ? A : C, A > C ? C : A);
+#pragma unroll
+          for (int q = 0; q < 10; ++q) J += I[q] * w[q];
+        }
+      } else if (sC == 0) {
+        J += blk_ptr(m, A > C ? A : C, A > C ? C : A)[pq] * w[0];
+      } else if (A >= C) {
+        const double* I = blk_ptr(m, A, C) + 10 * pq;
+#pragma unroll
+        for (int q = 0; q < 10; ++q) J += I[q] * w[q];
+      } else {
+        const double* I = blk_ptr(m, C, A) + pq;
+#pragma unroll
+        for (int q = 0; q < 10; ++q) J += I[10 * q] * w[q];
+      }
+    }
+    // one-center exchange -1/2 sum_{lam,sig in A} P_lam_sig (mu lam|nu sig)
+    double K = 0.0;
+    const int nA = nao_of_slot(sA);
+    for (int l = 0; l < nA; ++l)
+      for (int s = 0; s < nA; ++s) {
+        const double x = one_center_value(sA, a < l ? a : l, a < l ? l : a, b < s ? b : s, b < s ? s : b);
+        if (x != 0.0) K += m.P[pk(fA + l, fA + s)] * x;
+      }
+    const int i = fA + b, j = fA + a;  // i >= j
+    const int64_t ij = tri(i) + j;
+    const double h = m.H[ij], fv = h + (J - 0.5 * K);
+    m.F[ij] = fv;
+    if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
+    e += m.P[ij] * (h + fv) * (i == j ? 0.5 : 1.0);
+  }
+  // off-diagonal atom blocks: two-center exchange only
+  const int64_t np = tri(m.natoms);
+  for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
+    int A, B;
+    tri_inverse(p, A, B);
+    if (A == B) continue;
+    const int sA = m.slot[A], sB = m.slot[B], fA = m.first[A], fB = m.first[B];
+    const double* I = blk_ptr(m, A, B);
+    const int nA = nao_of_slot(sA), nB = nao_of_slot(sB);
+    double Pab[16];
+    for (int l = 0; l < nA; ++l)
+      for (int s = 0; s < nB; ++s) Pab[4 * l + s] = m.P[tri(fA + l) + fB + s];
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nB; ++nu) {
+        double g = 0.0;
+        if (sA != 0 && sB != 0) {
+          for (int l = 0; l < 4; ++l) {
+            const double* Ir = I + 10 * pair_index(mu, l);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) g += Pab[4 * l + s] * Ir[pair_index(nu, s)];
+          }
+        } else if (sA != 0) {  // B is H: (mu lam | s_B s_B), block column = pair(mu, lam)
+          for (int l = 0; l < 4; ++l) g += Pab[4 * l] * I[pair_index(mu, l)];
+        } else if (sB != 0) {  // A is H: (s_A s_A | nu sig)
+          for (int s = 0; s < 4; ++s) g += Pab[s] * I[pair_index(nu, s)];
+        } else {
+          g = Pab[0] * I[0];
+        }
+        const int i = fA + mu, j = fB + nu;
+        const int64_t ij = tri(i) + j;
+        const double h = m.H[ij], fv = h - 0.5 * g;
+        m.F[ij] = fv;
+        if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
+        e += m.P[ij] * (h + fv);
+      }
+  }
+  return block_sum<NT>(e, red);
+}
+
+// Initial guess P_ii = Z_A / nAO_A, zero elsewhere (densitymatrix.cpp:26-37).
+__device__ inline void block_guess(const MolView& m) {
+  const int64_t np = tri(m.nao);
+  for (int64_t t = threadIdx.x; t < np; t += blockDim.x) m.P[t] = 0.0;
+  __syncthreads();
+  for (int A = threadIdx.x; A < m.natoms; A += blockDim.x) {
+    const int s = m.slot[A], n = nao_of_slot(s), f = m.first[A];
+    for (int k = 0; k < n; ++k) m.P[tri(f + k) + f + k] = (double)c_elem[s].core / n;
+  }
+}
+
+// Core-core repulsion, sum over A < B (corecorerepulsion.cpp:12-65).
+template <int NT>
+__device__ double block_core_core(const MolView& m, double* red) {
+  double e = 0.0;
+  const int64_t np = tri(m.natoms);
+  for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
+    int Bh, Al;  // Bh > Al
+    tri_inverse(p, Bh, Al);
+    if (Bh == Al) continue;
+    const int sa = m.slot[Al], sb = m.slot[Bh];
+    const double gam = *blk_ptr(m, Bh, Al);
+    const double* pa = m.pos + 3 * Al;
+    const double* pb = m.pos + 3 * Bh;
+    const double dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+    const double r = sqrt(dx * dx + dy * dy + dz * dz) * kBohr2Ang;
+    const int za = c_elem[sa].z, zb = c_elem[sb].z;
+    double f;
+    if (zb == 1 && (za == 7 || za == 8))
+      f = 1.0 + r * exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
+    else if (za == 1 && (zb == 7 || zb == 8))
+      f = 1.0 + r * exp(-c_elem[sb].alpha * r) + exp(-c_elem[sa].alpha * r);
+    else
+      f = 1.0 + exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
+    e += (double)(c_elem[sa].core * c_elem[sb].core) * gam * f;
+  }
+  return block_sum<NT>(e, red);
+}
+
+// ------------------------------------------------------------------------------------------
+// Small dense helpers on one CTA.
+
+// C (smem or global, ldc) = op(A) * B with 4x4 register tiles; A is n x n (lda), B n x n (ldb).
+// transA: use A^T.
+template <bool TRANS_A>
+__device__ inline void block_gemm(int n, const double* A, int lda, const double* B, int ldb,
+                                  double* C, int ldc) {
+  const int tiles = (n + 3) >> 2;
+  for (int t = threadIdx.x; t < tiles * tiles; t += blockDim.x) {
+    const int i0 = (t / tiles) * 4, j0 = (t % tiles) * 4;
+    double acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+    for (int k = 0; k < n; ++k) {
+      double a[4], b[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int i = i0 + r < n ? i0 + r : n - 1;
+        a[r] = TRANS_A ? A[k * lda + i] : A[i * lda + k];
+      }
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int j = j0 + c < n ? j0 + c : n - 1;
+        b[c] = B[k * ldb + j];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (i0 + r < n && j0 + c < n) C[(i0 + r) * ldc + j0 + c] = acc[r][c];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Two-sided cyclic Jacobi on the symmetric matrix As (shared, n x n, ld) with the rotations
+// accumulated into V (global, n x n row-major): As <- G^T As G, V <- V G.  Parallel
+// round-robin ordering: with ne = n rounded up to even and m = ne - 1, round r pairs index m
+// with r and (r + k) % m with (r - k) % m for k = 1 .. ne/2 - 1; an index >= n is a dummy
+// (identity rotation).  Sweeps stop when the off-diagonal Frobenius norm falls below
+// rel_tol * ||A||_F.  Returns the number of sweeps, or -1 if max_sweeps was reached.
+struct JacobiScratch {
+  double* c;     // ne/2
+  double* s;     // ne/2
+  double* t;     // ne/2
+  double* red;   // 32
+};
+
+__device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
+  if (k == 0) { p = m; q = r; }
+  else { p = (r + k) % m; q = (r - k + m) % m; }
+}
+
+template <int NT>
+__device__ int block_jacobi(int n, double* As, int ld, double* V, JacobiScratch js,
+                            double rel_tol, int max_sweeps) {
+  const int ne = n + (n & 1), m = ne - 1, n2 = ne / 2;
+  double fro2 = 0.0;
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+    const double x = As[(t / n) * ld + t % n];
+    fro2 += x * x;
+  }
+  fro2 = block_sum<NT>(fro2, js.red);
+  const double tol2 = rel_tol * rel_tol * fro2;
+  for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+    double off = 0.0;
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+      const int i = t / n, j = t % n;
+      if (i != j) { const double x = As[i * ld + j]; off += x * x; }
+    }
+    off = block_sum<NT>(off, js.red);
+    if (off != off || fro2 != fro2) return -1;
+    if (off <= tol2) return sweep;
+    for (int r = 0; r < m; ++r) {
+      // rotations of this round
+      for (int k = threadIdx.x; k < n2; k += blockDim.x) {
+        int p, q;
+        rr_pair(r, k, m, p, q);
+        double c = 1.0, s = 0.0, t = 0.0;
+        if (p < n && q < n) {
+          const double apq = As[p * ld + q];
+          if (apq != 0.0) {
+            const double theta = (As[q * ld + q] - As[p * ld + p]) / (2.0 * apq);
+            const double at = fabs(theta);
+            t = at > 1e150 ? 0.5 / theta
+                           : (theta >= 0.0 ? 1.0 : -1.0) / (at + sqrt(fma(theta, theta, 1.0)));
+            c = 1.0 / sqrt(fma(t, t, 1.0));
+            s = t * c;
+          }
+        }
+        js.c[k] = c; js.s[k] = s; js.t[k] = t;
+      }
+      __syncthreads();
+      // As <- G^T As G, one 2x2 block (ka, kb) per task
+      for (int task = threadIdx.x; task < n2 * n2; task += blockDim.x) {
+        const int ka = task / n2, kb = task % n2;
+        int pa, qa, pb, qb;
+        rr_pair(r, ka, m, pa, qa);
+        rr_pair(r, kb, m, pb, qb);
+        if (ka == kb) {
+          if (pa < n && qa < n) {
+            const double apq = As[pa * ld + qa], tt = js.t[ka];
+            if (tt != 0.0) {
+              As[pa * ld + pa] -= tt * apq;
+              As[qa * ld + qa] += tt * apq;
+              As[pa * ld + qa] = 0.0;
+              As[qa * ld + pa] = 0.0;
+            }
+          }
+          continue;
+        }
+        const double ca = js.c[ka], sa = js.s[ka], cb = js.c[kb], sb = js.s[kb];
+        const bool vpa = pa < n, vqa = qa < n, vpb = pb < n, vqb = qb < n;
+        const double x00 = (vpa && vpb) ? As[pa * ld + pb] : 0.0;
+        const double x01 = (vpa && vqb) ? As[pa * ld + qb] : 0.0;
+        const double x10 = (vqa && vpb) ? As[qa * ld + pb] : 0.0;
+        const double x11 = (vqa && vqb) ? As[qa * ld + qb] : 0.0;
+        // rows: p' = c p - s q, q' = s p + c q
+        const double y00 = ca * x00 - sa * x10, y01 = ca * x01 - sa * x11;
+        const double y10 = sa * x00 + ca * x10, y11 = sa * x01 + ca * x11;
+        // columns
+        if (vpa && vpb) As[pa * ld + pb] = cb * y00 - sb * y01;
+        if (vpa && vqb) As[pa * ld + qb] = sb * y00 + cb * y01;
+        if (vqa && vpb) As[qa * ld + pb] = cb * y10 - sb * y11;
+        if (vqa && vqb) As[qa * ld + qb] = sb * y10 + cb * y11;
+      }
+      // V <- V G: task (row i, pair k)
+      for (int task = threadIdx.x; task < n * n2; task += blockDim.x) {
+        const int i = task / n2, k = task % n2;
+        int p, q;
+        rr_pair(r, k, m, p, q);
+        if (p >= n || q >= n) continue;
+        const double c = js.c[k], s = js.s[k];
+        if (s == 0.0) continue;
+        double* row = V + (int64_t)i * n;
+        const double vp = row[p], vq = row[q];
+        row[p] = c * vp - s * vq;
+        row[q] = s * vp + c * vq;
+      }
+      __syncthreads();
+    }
+  }
+  return -1;
+}
+
+}  // namespace sgb

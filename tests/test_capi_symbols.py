@@ -1,0 +1,44 @@
+"""The C ABI library loads without a GPU and exports every entry point declared in
+include/semigpu_b200.h; no compute call is made here."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "semigpu_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sgb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert "sgb_scf" in names and "sgb_batch_run" in names and len(names) >= 20
+
+
+def test_library_exports_every_symbol():
+    import semigpu_b200 as sg
+
+    if not os.path.exists(sg.LIB_PATH):
+        from semigpu_b200 import build as _b
+
+        _b.build()
+    L = ctypes.CDLL(sg.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(L, n)]
+    assert not missing, missing
+    assert set(sg.SIGNATURES) == set(declared())
+
+
+def test_status_strings_without_gpu():
+    import semigpu_b200 as sg
+
+    L = sg.lib()
+    assert L.sgb_status_string(0) == b"ok"
+    assert L.sgb_status_string(-2).startswith(b"element")
