@@ -1,0 +1,414 @@
+"""Benchmark: converged SCF molecules/s on the 4096-molecule uneven batch (FP64, tol 1e-6 eV).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one persistent launch that takes every molecule of the batch from coordinates to
+converged total energy (integrals, Hcore, SCF, core-core).  `value` is device-timed
+(CUDA events recorded by the library around each launch, inputs resident in HBM);
+`e2e` goes through the public C ABI (sgb_run_molecules) from pinned host arrays with the
+coordinate upload and the result read-back inside the timed region.  Multi-GPU: one process
+per GPU under torchrun, each rank runs its own seeded 4096-molecule batch (weak scaling, no
+collective on the data path); time is the max over ranks.
+
+--impl reference times the reference's own CPU build (oracle/_ref/ref_driver, the unmodified
+LuisAlfredoNu/semiGPU sources compiled serially) on bounded samples of the same workload, one
+molecule per process on all host cores; rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "converged SCF molecules/s + p50/p99 latency vs plain FP64 GPU, |ΔE|≤1e-4 eV"
+UNIT = "molecules/s"
+BATCH = 4096
+TOL = 1e-6
+WORKLOAD = ("uneven batch of 4096 seeded molecules per GPU: 50% CnH2n+2 (n=1..20), 30% all-trans "
+            "CnHn+2 (n even 2..30), 20% aza-aromatic rings (0-3 N); coordinates jittered "
+            "N(0,0.01 A); FP64; SCF to |dE| < 1e-6 eV")
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+# ------------------------------------------------------------------------------------------
+# Clock sampling during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------------------------------
+# Algorithmic work (the roofline numerator)
+
+def algorithmic_flops(mols, n_iter) -> float:
+    """Per SCF step and molecule: eigensolve (10/3) N^3 (Householder tridiagonalisation +
+    back-transform, independent of the algorithm run) + density 2 N^2 nocc; summed over the
+    steps each molecule took."""
+    tot = 0.0
+    for m, it in zip(mols, n_iter):
+        n, o = m.nao, m.nocc
+        tot += float(it) * ((10.0 / 3.0) * n ** 3 + 2.0 * n * n * o)
+    return tot
+
+
+def fp64_peak_tflops(torch):
+    """Measured cuBLAS DGEMM throughput (the FP64 peak the roofline is quoted against);
+    cached in profiles/fp64_peak.json once measured on this pool."""
+    path = os.path.join(ROOT, "profiles", "fp64_peak.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)["dgemm_tflops"], "profiles/fp64_peak.json (measured cuBLAS DGEMM)"
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(); a @ b; e1.record(); torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return 2 * n ** 3 / best / 1e12, "measured in this run (cuBLAS DGEMM 8192^3, best of 5)"
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "k_batch_scf_traffic.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return None
+
+
+# ------------------------------------------------------------------------------------------
+# CPU reference timing
+
+def stratified(mols, k, offset=0):
+    """k molecules at evenly spaced quantiles of nao, largest first (so a process pool
+    schedules them longest-job-first)."""
+    idx = np.argsort([m.nao for m in mols], kind="stable")
+    pos = np.linspace(0, len(mols) - 1, k).round().astype(int)
+    pos = np.clip(pos + offset, 0, len(mols) - 1)
+    return [mols[int(idx[p])] for p in pos[::-1]]
+
+
+def _ref_one(args):
+    Z, xyz = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    r = oracle.run_reference(Z, xyz, tol=TOL, matrices=False)
+    return r["E_tot"], r["n_iter"]
+
+
+def time_reference(sample, cores):
+    """Wall time of the reference CLI engine over `sample`, one molecule per process."""
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(min(cores, len(sample))) as pool:
+        out = pool.map(_ref_one, [(m.Z, m.xyz) for m in sample], chunksize=1)
+    return time.perf_counter() - t0, out
+
+
+def reference_kind():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    return "reference" if oracle.reference_available() else None
+
+
+# ------------------------------------------------------------------------------------------
+
+def run_reference_arm(args):
+    from semigpu_b200 import geometry as geo
+
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return
+    if reference_kind() is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_driver not built (the reference tree was absent when "
+                          "oracle/Makefile ran)"}))
+        return
+    mols = geo.batch_c3(BATCH, seed=0)
+    cores = os.cpu_count() or 1
+    per_step = max(cores, 8)
+    times, done = [], 0
+    small = sorted(mols, key=lambda m: m.nao)[: len(mols) // 4]
+    for s in range(args.warmup + args.steps):
+        # warm-up steps run a light sample (process-pool start-up, page cache)
+        sample = stratified(small if s < args.warmup else mols, per_step, offset=s)
+        dt, _ = time_reference(sample, cores)
+        if s >= args.warmup:
+            times.append(dt)
+            done += len(sample)
+    total = sum(times)
+    value = done / total
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample_per_step": per_step,
+                   "sample": "stratified by nao over the seed-0 batch, shifted each step"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{per_step} molecules per step, stratified by nao"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import semigpu_b200 as sg
+    from semigpu_b200 import geometry as geo
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    nb = args.batch
+    mols = geo.batch_c3(nb, seed=rank)
+    ctx = sg.Context(local)
+    batch = sg.Batch(ctx, mols)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        ctx.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        batch.run(TOL)
+        res = batch.results()
+    barrier()
+    kernel_ms = []
+    lat_p50, lat_p99 = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            batch.run(TOL)
+            res = batch.results()
+            kernel_ms.append(batch.last_ms())
+            tb, te = batch.timestamps()
+            lat = (te.astype(np.float64) - float(tb.min())) / 1e6
+            lat_p50.append(float(np.percentile(lat, 50)))
+            lat_p99.append(float(np.percentile(lat, 99)))
+        barrier()
+    clk = clocks.summary()
+    my_ms = float(sum(kernel_ms))
+    t = torch.tensor([my_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ok = bool(np.all(res["status"] == 0) and np.all(res["converged"]))
+    value = world * nb * args.steps / (total_ms / 1e3)
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                              "steps": args.steps, "warmup": args.warmup,
+                              "ms_per_step": total_ms / args.steps, "kernel_only": True,
+                              "molecules_per_gpu": nb, "all_converged": ok, "clocks": clk}))
+        batch.close()
+        ctx.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    # e2e through the C ABI from pinned host memory: upload coordinates, run, read results
+    natoms = np.array([m.natoms for m in mols], np.int32)
+    rng = np.random.default_rng(100 + rank)
+    pinned = torch.empty(int(natoms.sum()) * 3, dtype=torch.float64).pin_memory().numpy()
+    base = np.concatenate([m.xyz.reshape(-1) for m in mols])
+    e2e_mols = [geo.Molecule(m.Z, m.xyz) for m in mols]
+    sg.run_molecules(ctx, e2e_mols, tol=TOL)  # builds the cached device batch
+    barrier()
+    e2e_s = 0.0
+    for _ in range(args.steps):
+        pinned[:] = base + rng.normal(0.0, 1e-4, base.shape)
+        off = 0
+        for m in e2e_mols:
+            k = m.natoms * 3
+            m.xyz = pinned[off:off + k].reshape(-1, 3)
+            off += k
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        r = sg.run_molecules(ctx, e2e_mols, tol=TOL)
+        e2e_s += time.perf_counter() - t0
+    te2e = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te2e, op=dist.ReduceOp.MAX)
+    e2e_value = world * nb * args.steps / float(te2e.item())
+    ok = ok and bool(np.all(r["status"] == 0))
+
+    if rank == 0:
+        peak, peak_src = fp64_peak_tflops(torch)
+        flops = algorithmic_flops(mols, res["n_iter"])
+        achieved = flops / (my_ms / args.steps / 1e3) / 1e12
+        traffic = load_traffic()
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None, "kernel": "k_batch_scf<512>",
+                "peak_source": peak_src,
+                "numerator": "sum over molecules of n_iter*((10/3)N^3 + 2 N^2 nocc) FP64 flops"}
+        if traffic:
+            roof["traffic"] = traffic["dram_bytes_per_molecule"] * nb
+            roof["traffic_source"] = traffic["source"]
+        # plain FP64 GPU path: one molecule at a time through the stage API (same kernels,
+        # one CTA per launch), on a stratified sample
+        sample = stratified(mols, 48)
+        tp = time.perf_counter()
+        plain_lat = []
+        for m in sample:
+            t1 = time.perf_counter()
+            sg.Molecule.from_geometry(ctx, m).run(tol=TOL)
+            plain_lat.append(time.perf_counter() - t1)
+        plain = len(sample) / (time.perf_counter() - tp)
+        # CPU baseline: the reference build on the host cores, bounded sample
+        cpu = None
+        if reference_kind():
+            cores = os.cpu_count() or 1
+            csample = stratified(mols, max(16, min(cores, 32)))
+            dt, _ = time_reference(csample, cores)
+            cpu = {"value": len(csample) / dt, "unit": UNIT, "cores": min(cores, len(csample)),
+                   "kind": "reference",
+                   "sample": f"{len(csample)} molecules stratified by nao from the same batch, "
+                             f"one reference process per molecule ({dt:.1f} s wall)"}
+        nat_total = int(natoms.sum())
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "molecules_per_gpu": nb, "tol_eV": TOL,
+                       "precision": "fp64", "parallelism": f"replicas x{world}",
+                       "l2": "working set > L2 (integrals + eigenvector arenas); a 256 MB "
+                             "buffer is written between timed steps"},
+            "latency_ms": {"p50": statistics.median(lat_p50), "p99": statistics.median(lat_p99),
+                           "definition": "per-molecule time from launch start to its converged "
+                                         "energy, device clock"},
+            "plain_fp64_gpu": {"value": plain, "unit": UNIT,
+                               "p50_ms": 1e3 * statistics.median(plain_lat),
+                               "p99_ms": 1e3 * float(np.percentile(plain_lat, 99)),
+                               "sample": "48 molecules stratified by nao, one molecule per call "
+                                         "through the stage API"},
+            "speedup_vs_plain_fp64_gpu": value / plain,
+            "all_converged": ok,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * nat_total,
+                    "d2h_bytes_per_step": nb * (8 + 8 + 4 + 4 + 4)},
+            "clocks": clk,
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line))
+    batch.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch", type=int, default=BATCH,
+                    help="molecules per GPU (default: the 4096-molecule workload)")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="device-timed launches only (no e2e, plain-path or CPU legs); used "
+                         "for profiler captures of a smaller batch")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -116,6 +116,11 @@ int sgb_run_molecules(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, c
                       int *converged, int *status);
 /* Device-time of the last sgb_batch_run in milliseconds (CUDA events on the context stream). */
 int sgb_batch_last_ms(const sgb_batch *b, float *ms);
+/* Per-molecule device timestamps (ns, %globaltimer) of the last run: when its CTA started the
+ * molecule and when its energies were written.  Latency of molecule m inside the launch:
+ * t_end[m] - min(t_begin). */
+int sgb_batch_timestamps(sgb_ctx *ctx, sgb_batch *b, unsigned long long *t_begin,
+                         unsigned long long *t_end);
 /* Device pointer of the batch's coordinate buffer (natoms_total*3 doubles) for callers that
  * stage inputs themselves. */
 int sgb_batch_device_coordinates(sgb_batch *b, void **dptr);

@@ -55,6 +55,8 @@ SIGNATURES = {
                                          ctypes.c_int, _D, _D, _I, _I, _I]),
     "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
     "sgb_batch_device_coordinates": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
+    "sgb_batch_timestamps": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_ulonglong),
+                                            ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 _lib = None
@@ -248,6 +250,15 @@ class Batch:
         ms = ctypes.c_float()
         lib().sgb_batch_last_ms(self.h, ctypes.byref(ms))
         return ms.value
+
+    def timestamps(self):
+        """(t_begin, t_end) per molecule in ns of the device clock, last run."""
+        tb = np.zeros(self.nmol, np.uint64)
+        te = np.zeros(self.nmol, np.uint64)
+        P = ctypes.POINTER(ctypes.c_ulonglong)
+        self.ctx.check(lib().sgb_batch_timestamps(self.ctx.h, self.h, tb.ctypes.data_as(P),
+                                                  te.ctypes.data_as(P)), "timestamps")
+        return tb, te
 
     def device_coordinates(self) -> int:
         p = _VP()

@@ -3,16 +3,16 @@
 // Molecules are handed out in the order given by `order` (the host sorts by estimated cost,
 // largest first, so the tail of the launch holds the cheap ones).
 //
-// Shared memory holds the n x n Fock/Jacobi matrix (odd leading dimension, so a column walk
-// does not hit one bank), the per-atom pair densities, the Jacobi rotation parameters and a
-// few reduction slots.  Eigenvectors, Hcore, P and F live in global memory (L2-resident at
-// these sizes).
+// Shared memory holds the eigensolver's working matrix G = (F + mu I) V (odd leading
+// dimension) and, for nao <= 110, the eigenvectors V as well; the per-atom pair densities and a
+// few reduction slots follow.  Hcore, P, F (packed and full) live in global memory
+// (L2-resident at these sizes), as does V for the larger molecules.
 //
 // The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
 // repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
-// max_iter steps.  The eigensolve after the first step is warm-started: the previous
-// eigenvectors V nearly diagonalise the new F, so Jacobi runs on V^T F V with V as the initial
-// accumulated rotation, and converges in one or two sweeps.
+// max_iter steps.  The eigensolve is a one-sided Jacobi on (F + mu I) V; after the first step
+// it is warm-started from the previous eigenvectors, whose columns the new F barely mixes, so
+// it converges in one or two sweeps.
 #pragma once
 #include "scf_block.cuh"
 
@@ -45,9 +45,18 @@ struct BatchArgs {
   double tol;
   int max_iter;
   int nmax;         // largest nao in the launch (sizes the shared memory)
+  size_t mat_doubles;  // shared matrix region (max over molecules of mat_doubles_for)
   int sorted_vectors;
   int stages;       // STAGE_* bits
+  unsigned long long* t_begin;  // optional per-molecule %globaltimer (ns) at start / end
+  unsigned long long* t_end;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 enum : int { STAGE_INTS = 1, STAGE_HCORE = 2, STAGE_SCF = 4, STAGE_CC = 8, STAGE_ALL = 15,
              STAGE_FOCK = 16 /* F and E_el from the P already in device memory */ };
@@ -56,13 +65,18 @@ enum : int { MOL_OK = 0, MOL_EIG_FAILED = 1, MOL_NAN = 2 };
 
 __host__ __device__ inline int smem_ld(int n) { return n | 1; }
 
-// Shared memory doubles for a launch whose largest molecule has nao = nmax.
-__host__ __device__ inline size_t batch_smem_doubles(int nmax) {
-  const size_t ld = (size_t)smem_ld(nmax);
-  const size_t ne2 = (size_t)(nmax + 2) / 2;
-  return (size_t)nmax * ld      // As
-         + 3 * (size_t)nmax + 8  // wq (<= 2.5 n) + pad
-         + 3 * ne2               // Jacobi c, s, t
+// Shared memory plan.  The matrix region holds G (n x ld, column-major) and, when it fits, the
+// eigenvectors V (n x ld) too; otherwise V stays in global memory.  The region size is fixed
+// per launch (mat_doubles); the small arrays follow it.
+constexpr int kVsmemMax = 110;  // 2 * 110 * 111 doubles = 195 KB: G and V both in smem
+
+__host__ __device__ inline size_t mat_doubles_for(int n) {
+  const size_t ld = (size_t)smem_ld(n);
+  return (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
+}
+
+__host__ __device__ inline size_t extra_doubles(int nmax) {
+  return 3 * (size_t)nmax + 8   // wq (<= 2.5 n) + pad
          + (size_t)nmax          // eigenvalues of the last eigensolve
          + 32                    // reductions
          + (size_t)nmax / 2 + 1; // occupied index list (ints, two per double)
@@ -83,8 +97,8 @@ __device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& 
   return v;
 }
 
-// P (packed) = 2 Vo Vo^T with Vo = n x nocc in shared memory (ldo), 4x4 register tiles on the
-// lower triangle of tiles.
+// P (packed) = 2 Vo Vo^T with Vo = nocc column vectors (column-major, ldo) in shared memory;
+// 4x4 register tiles over the lower triangle of tiles.
 __device__ inline void block_density(int n, int nocc, const double* Vo, int ldo, double* P) {
   const int tiles = (n + 3) >> 2;
   const int ntile = tiles * (tiles + 1) / 2;
@@ -103,11 +117,12 @@ __device__ inline void block_density(int n, int nocc, const double* Vo, int ldo,
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
     for (int k = 0; k < nocc; ++k) {
+      const double* col = Vo + (int64_t)k * ldo;
       double a[4], b[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = i0 + r < n ? Vo[(i0 + r) * ldo + k] : 0.0;
+      for (int r = 0; r < 4; ++r) a[r] = i0 + r < n ? col[i0 + r] : 0.0;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = j0 + c < n ? Vo[(j0 + c) * ldo + k] : 0.0;
+      for (int c = 0; c < 4; ++c) b[c] = j0 + c < n ? col[j0 + c] : 0.0;
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -123,22 +138,33 @@ __device__ inline void block_density(int n, int nocc, const double* Vo, int ldo,
   }
 }
 
+// rank of dval[i] in ascending order (ties by index)
+__device__ __forceinline__ int ascending_rank(const double* dval, int n, int i) {
+  const double di = dval[i];
+  int rank = 0;
+  for (int j = 0; j < n; ++j) {
+    const double dj = dval[j];
+    rank += (dj < di) || (dj == di && j < i);
+  }
+  return rank;
+}
+
 template <int NT>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
   const MolView m = make_view(a, d);
   const int n = m.nao, ld = smem_ld(n);
   const size_t nmax = (size_t)a.nmax;
-  double* As = smem;
-  double* wq = As + nmax * smem_ld(a.nmax);
-  double* jc = wq + 3 * nmax + 8;
-  const size_t ne2 = (nmax + 2) / 2;
-  double* js_ = jc + ne2;
-  double* jt = js_ + ne2;
-  double* dval = jt + ne2;
+  const bool v_smem = mat_doubles_for(n) == 2 * (size_t)n * ld;
+  double* G = smem;
+  double* V = v_smem ? smem + (size_t)n * ld : m.V;
+  const int ldv = v_smem ? ld : n;
+  double* wq = smem + a.mat_doubles;
+  double* dval = wq + 3 * nmax + 8;
   double* red = dval + nmax;
   int* occ = reinterpret_cast<int*>(red + 32);
-  JacobiScratch js{jc, js_, jt, red};
+  double* Ffull = m.T;  // F as a full n x n matrix, global scratch
+  if (a.t_begin && threadIdx.x == 0) a.t_begin[mi] = global_ns();
 
   if (a.stages & STAGE_INTS) {
     block_integrals(m);
@@ -153,72 +179,55 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   if (a.stages & STAGE_SCF) {
     block_guess(m);
     __syncthreads();
-    E = block_fock_energy<NT>(m, As, ld, wq, red);
+    E = block_fock_energy<NT>(m, Ffull, n, wq, red);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     while (!conv && steps < a.max_iter) {
-      // ---- eigensolve of F (in As) ----
+      // ---- eigensolve of F: one-sided Jacobi on (F + mu I) V, V warm-started ----
+      const double mu = block_shift<NT>(n, Ffull, red);
       if (steps == 0) {
-        for (int t = threadIdx.x; t < n * n; t += blockDim.x)
-          m.V[t] = (t / n == t % n) ? 1.0 : 0.0;
-      } else {
-        block_gemm<false>(n, As, ld, m.V, n, m.T, n);  // T = F V
-        __syncthreads();
-        block_gemm<true>(n, m.V, n, m.T, n, As, ld);   // As = V^T T
-        __syncthreads();
         for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-          const int i = t / n, j = t % n;
-          if (i < j) {
-            const double s = 0.5 * (As[i * ld + j] + As[j * ld + i]);
-            As[i * ld + j] = s;
-            As[j * ld + i] = s;
-          }
+          const int j = t / n, i = t % n;
+          V[(int64_t)j * ldv + i] = i == j ? 1.0 : 0.0;
+          G[(int64_t)j * ld + i] = Ffull[t] + (i == j ? mu : 0.0);
         }
+      } else {
+        block_shifted_product(n, Ffull, mu, V, ldv, G, ld);
       }
       __syncthreads();
-      const int sw = block_jacobi<NT>(n, As, ld, m.V, js, 1e-14, 60);
+      const int sw = block_onesided_jacobi<NT>(n, G, ld, V, ldv, red, 1e-15, 1e-10, 40);
       if (sw < 0) { status = MOL_EIG_FAILED; break; }
-      // ---- eigenvalues, occupied set ----
-      for (int i = threadIdx.x; i < n; i += blockDim.x) dval[i] = As[i * ld + i];
+      block_rayleigh<NT>(n, G, ld, V, ldv, mu, dval);
       __syncthreads();
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double di = dval[i];
-        int rank = 0;
-        for (int j = 0; j < n; ++j) {
-          const double dj = dval[j];
-          rank += (dj < di) || (dj == di && j < i);
-        }
+        const int rank = ascending_rank(dval, n, i);
         if (rank < m.nocc) occ[rank] = i;
       }
       __syncthreads();
-      // ---- density from the occupied vectors (gathered into shared memory) ----
-      const int ldo = m.nocc | 1;
+      // ---- density from the occupied vectors, gathered into the G region ----
       for (int t = threadIdx.x; t < n * m.nocc; t += blockDim.x) {
-        const int i = t / m.nocc, k = t % m.nocc;
-        As[i * ldo + k] = m.V[(int64_t)i * n + occ[k]];
+        const int k = t / n, i = t % n;
+        G[(int64_t)k * ld + i] = V[(int64_t)occ[k] * ldv + i];
       }
       __syncthreads();
-      block_density(n, m.nocc, As, ldo, m.P);
+      block_density(n, m.nocc, G, ld, m.P);
       __syncthreads();
       // ---- Fock + energy ----
       const double Eold = E;
-      E = block_fock_energy<NT>(m, As, ld, wq, red);
+      E = block_fock_energy<NT>(m, Ffull, n, wq, red);
       ++steps;
       if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride + steps] = E;
       if (E != E) { status = MOL_NAN; break; }
       conv = fabs(Eold - E) < a.tol;
     }
-    // eigenvalues (ascending) and, on request, eigenvectors sorted the same way into T
+    // eigenvalues (ascending) and, on request, the eigenvectors sorted the same way into T
+    // (column k = vector k, the layout of SCFCalculation::eigenVec)
     if (steps > 0) {
+      __syncthreads();
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const double di = dval[i];
-        int rank = 0;
-        for (int j = 0; j < n; ++j) {
-          const double dj = dval[j];
-          rank += (dj < di) || (dj == di && j < i);
-        }
-        m.eig[rank] = di;
+        const int rank = ascending_rank(dval, n, i);
+        m.eig[rank] = dval[i];
         if (a.sorted_vectors)
-          for (int r = 0; r < n; ++r) m.T[(int64_t)r * n + rank] = m.V[(int64_t)r * n + i];
+          for (int r = 0; r < n; ++r) m.T[(int64_t)rank * n + r] = V[(int64_t)i * ldv + r];
       }
     }
   }
@@ -236,6 +245,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       a.status[mi] = status;
     }
     if (a.stages & STAGE_CC) a.e_cc[mi] = ecc;
+    if (a.t_end) a.t_end[mi] = global_ns();
   }
   __syncthreads();
 }

@@ -67,6 +67,7 @@ struct sgb_batch {
   double *d_V = nullptr, *d_T = nullptr, *d_eig = nullptr;
   double *d_eel = nullptr, *d_ecc = nullptr;
   int *d_niter = nullptr, *d_conv = nullptr, *d_status = nullptr;
+  unsigned long long *d_tb = nullptr, *d_te = nullptr;
   double* d_hist = nullptr;
   int hist_stride = 0;
   int64_t n_ints = 0, n_pk = 0, n_sq = 0, n_ao = 0;
@@ -196,7 +197,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
                o_P = take(8 * b->n_pk), o_F = take(8 * b->n_pk), o_V = take(8 * b->n_sq),
                o_T = take(8 * b->n_sq), o_eig = take(8 * b->n_ao), o_eel = take(8 * nmol),
                o_ecc = take(8 * nmol), o_nit = take(4 * nmol), o_conv = take(4 * nmol),
-               o_stat = take(4 * nmol),
+               o_stat = take(4 * nmol), o_tb = take(8 * nmol), o_te = take(8 * nmol),
                o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0);
   b->bytes = off;
   if (ctx->budget && ctx->in_use + off > ctx->budget) {
@@ -232,6 +233,8 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->d_niter = (int*)(base + o_nit);
   b->d_conv = (int*)(base + o_conv);
   b->d_status = (int*)(base + o_stat);
+  b->d_tb = (unsigned long long*)(base + o_tb);
+  b->d_te = (unsigned long long*)(base + o_te);
   b->d_hist = hist_stride > 0 ? (double*)(base + o_hist) : nullptr;
   cudaStream_t st = ctx->stream;
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -283,10 +286,16 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.hist = b->d_hist; a.hist_stride = b->hist_stride;
   a.tol = tol;
   a.max_iter = std::min(max_iter, b->hist_stride > 0 ? b->hist_stride - 1 : max_iter);
-  a.nmax = std::max(1, std::min(b->nmax, kSmallNmax));
+  // stages without the SCF matrix still use the reduction slots of the shared layout
+  a.nmax = needs_smem ? std::max(1, b->nmax) : 1;
   a.sorted_vectors = sorted_vectors;
   a.stages = stages;
-  const size_t smem = needs_smem ? batch_smem_doubles(a.nmax) * sizeof(double) : 0;
+  a.t_begin = b->d_tb;
+  a.t_end = b->d_te;
+  a.mat_doubles = 0;
+  if (needs_smem)
+    for (const MolDesc& d : b->desc) a.mat_doubles = std::max(a.mat_doubles, mat_doubles_for(d.nao));
+  const size_t smem = (a.mat_doubles + extra_doubles(a.nmax)) * sizeof(double);
   cudaStream_t st = ctx->stream;
   CUDA_TRY(ctx, cudaFuncSetAttribute(k_batch_scf<kThreads>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -480,17 +489,6 @@ int sgb_get(sgb_ctx* ctx, const sgb_mol* mol, int which, double* host, size_t co
     default: return fail(ctx, SGB_E_ARG, "unknown matrix id %d", which);
   }
   if (count < need) return fail(ctx, SGB_E_ARG, "buffer holds %zu, need %zu", count, need);
-  if (which == SGB_EIGVEC) {
-    // device T is row-major sorted vectors (T[r*n + k]); the reference's eigenVec is
-    // column-major, i.e. the transpose in row-major terms
-    std::vector<double> tmp(need);
-    CUDA_TRY(ctx, cudaMemcpyAsync(tmp.data(), src, 8 * need, cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    const int n = d.nao;
-    for (int r = 0; r < n; ++r)
-      for (int k = 0; k < n; ++k) host[(size_t)k * n + r] = tmp[(size_t)r * n + k];
-    return SGB_OK;
-  }
   CUDA_TRY(ctx, cudaMemcpyAsync(host, src, 8 * need, cudaMemcpyDeviceToHost, ctx->stream));
   return sgb_ctx_synchronize(ctx);
 }
@@ -544,6 +542,15 @@ int sgb_batch_last_ms(const sgb_batch* b, float* ms) {
   if (!b || !ms) return SGB_E_ARG;
   *ms = b->last_ms;
   return SGB_OK;
+}
+
+int sgb_batch_timestamps(sgb_ctx* ctx, sgb_batch* b, unsigned long long* t_begin,
+                         unsigned long long* t_end) {
+  if (!ctx || !b) return SGB_E_ARG;
+  const size_t n = (size_t)b->nmol;
+  if (t_begin) CUDA_TRY(ctx, cudaMemcpyAsync(t_begin, b->d_tb, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  if (t_end) CUDA_TRY(ctx, cudaMemcpyAsync(t_end, b->d_te, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return sgb_ctx_synchronize(ctx);
 }
 
 int sgb_batch_device_coordinates(sgb_batch* b, void** dptr) {

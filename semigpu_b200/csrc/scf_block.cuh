@@ -171,7 +171,7 @@ __device__ inline void block_hcore(const MolView& m) {
 
 // ------------------------------------------------------------------------------------------
 // Fock build + electronic energy.  Writes F packed to global memory and, when Fs != nullptr,
-// the full symmetric F into shared memory (leading dimension ld).  Returns E_el in every thread.
+// the full symmetric F (leading dimension ld).  Returns E_el in every thread.
 //
 // wq: shared scratch of 10 * nheavy + nlight doubles: the pair densities of each atom,
 //     w_C[q] = P_{lam sig} (x2 when lam != sig) for pair q = (lam, sig) of atom C.
@@ -315,155 +315,190 @@ __device__ double block_core_core(const MolView& m, double* red) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Small dense helpers on one CTA.
+// Dense helpers on one CTA.
 
-// C (smem or global, ldc) = op(A) * B with 4x4 register tiles; A is n x n (lda), B n x n (ldb).
-// transA: use A^T.
-template <bool TRANS_A>
-__device__ inline void block_gemm(int n, const double* A, int lda, const double* B, int ldb,
-                                  double* C, int ldc) {
+template <int NT>
+__device__ __forceinline__ double block_max(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (l < NT / 32) ? red[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (l == 0) red[0] = v;
+  }
+  __syncthreads();
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Shift making F + mu I positive semi-definite: mu = ||F||_inf + 1 (row sums of |F_ij|).
+template <int NT>
+__device__ double block_shift(int n, const double* Ffull, double* red) {
+  double mx = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double s = 0.0;
+    const double* row = Ffull + (int64_t)i * n;
+    for (int j = 0; j < n; ++j) s += fabs(row[j]);
+    mx = fmax(mx, s);
+  }
+  return block_max<NT>(mx, red) + 1.0;
+}
+
+// G (column-major, ldg) = (F + mu I) V with F full symmetric (row-major = column-major, n x n,
+// ld n) and V column-major (ldv); 4x4 register tiles.
+__device__ inline void block_shifted_product(int n, const double* F, double mu, const double* V,
+                                             int ldv, double* G, int ldg) {
   const int tiles = (n + 3) >> 2;
   for (int t = threadIdx.x; t < tiles * tiles; t += blockDim.x) {
-    const int i0 = (t / tiles) * 4, j0 = (t % tiles) * 4;
+    const int i0 = (t % tiles) * 4, j0 = (t / tiles) * 4;
     double acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-    for (int k = 0; k < n; ++k) {
+    const double* fr[4];
+    const double* vc[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) fr[r] = F + (int64_t)(i0 + r < n ? i0 + r : n - 1) * n;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) vc[c] = V + (int64_t)(j0 + c < n ? j0 + c : n - 1) * ldv;
+    for (int l = 0; l < n; ++l) {
       double a[4], b[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int i = i0 + r < n ? i0 + r : n - 1;
-        a[r] = TRANS_A ? A[k * lda + i] : A[i * lda + k];
-      }
+      for (int r = 0; r < 4; ++r) a[r] = fr[r][l];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int j = j0 + c < n ? j0 + c : n - 1;
-        b[c] = B[k * ldb + j];
-      }
+      for (int c = 0; c < 4; ++c) b[c] = vc[c][l];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c)
 #pragma unroll
-      for (int c = 0; c < 4; ++c)
-        if (i0 + r < n && j0 + c < n) C[(i0 + r) * ldc + j0 + c] = acc[r][c];
+      for (int r = 0; r < 4; ++r) {
+        const int i = i0 + r, j = j0 + c;
+        if (i < n && j < n) G[(int64_t)j * ldg + i] = fma(mu, vc[c][i], acc[r][c]);
+      }
   }
 }
 
 // ------------------------------------------------------------------------------------------
-// Two-sided cyclic Jacobi on the symmetric matrix As (shared, n x n, ld) with the rotations
-// accumulated into V (global, n x n row-major): As <- G^T As G, V <- V G.  Parallel
-// round-robin ordering: with ne = n rounded up to even and m = ne - 1, round r pairs index m
-// with r and (r + k) % m with (r - k) % m for k = 1 .. ne/2 - 1; an index >= n is a dummy
-// (identity rotation).  Sweeps stop when the off-diagonal Frobenius norm falls below
-// rel_tol * ||A||_F.  Returns the number of sweeps, or -1 if max_sweeps was reached.
-struct JacobiScratch {
-  double* c;     // ne/2
-  double* s;     // ne/2
-  double* t;     // ne/2
-  double* red;   // 32
-};
+// One-sided (Hestenes) cyclic Jacobi.  G = (F + mu I) V0 with V0 orthogonal; rotations from
+// the right orthogonalise the columns of G and are accumulated into V (both column-major).
+// With F + mu I positive semi-definite the converged V holds eigenvectors of F and
+// g_i . v_i - mu its eigenvalues.  A rotation touches two columns only, so one warp owns one
+// column pair of a round (columns held in registers, n <= 32 * kColRegs); rounds follow the
+// round-robin ordering (ne = n rounded up to even, m = ne - 1: round r pairs m with r and
+// (r + k) % m with (r - k) % m; an index >= n is a dummy).  A rotation is skipped when
+// |g_p.g_q| <= rot_tol sqrt(|g_p|^2 |g_q|^2); sweeps stop after one whose largest measured
+// off-diagonal cosine was below done_tol (the next would start from its square).  Returns the
+// sweep count, or -1 if max_sweeps ran out or a non-finite value appeared.
+constexpr int kColRegs = 5;  // n <= 160
 
 __device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
   if (k == 0) { p = m; q = r; }
-  else { p = (r + k) % m; q = (r - k + m) % m; }
+  else {
+    p = r + k; if (p >= m) p -= m;
+    q = r - k; if (q < 0) q += m;
+  }
 }
 
 template <int NT>
-__device__ int block_jacobi(int n, double* As, int ld, double* V, JacobiScratch js,
-                            double rel_tol, int max_sweeps) {
+__device__ int block_onesided_jacobi(int n, double* G, int ldg, double* V, int ldv, double* red,
+                                     double rot_tol, double done_tol, int max_sweeps) {
   const int ne = n + (n & 1), m = ne - 1, n2 = ne / 2;
-  double fro2 = 0.0;
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-    const double x = As[(t / n) * ld + t % n];
-    fro2 += x * x;
-  }
-  fro2 = block_sum<NT>(fro2, js.red);
-  const double tol2 = rel_tol * rel_tol * fro2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  constexpr int NW = NT / 32;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
-    double off = 0.0;
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-      const int i = t / n, j = t % n;
-      if (i != j) { const double x = As[i * ld + j]; off += x * x; }
-    }
-    off = block_sum<NT>(off, js.red);
-    if (off != off || fro2 != fro2) return -1;
-    if (off <= tol2) return sweep;
+    double worst = 0.0;
     for (int r = 0; r < m; ++r) {
-      // rotations of this round
-      for (int k = threadIdx.x; k < n2; k += blockDim.x) {
-        int p, q;
-        rr_pair(r, k, m, p, q);
-        double c = 1.0, s = 0.0, t = 0.0;
-        if (p < n && q < n) {
-          const double apq = As[p * ld + q];
-          if (apq != 0.0) {
-            const double theta = (As[q * ld + q] - As[p * ld + p]) / (2.0 * apq);
-            const double at = fabs(theta);
-            t = at > 1e150 ? 0.5 / theta
-                           : (theta >= 0.0 ? 1.0 : -1.0) / (at + sqrt(fma(theta, theta, 1.0)));
-            c = 1.0 / sqrt(fma(t, t, 1.0));
-            s = t * c;
-          }
-        }
-        js.c[k] = c; js.s[k] = s; js.t[k] = t;
-      }
-      __syncthreads();
-      // As <- G^T As G, one 2x2 block (ka, kb) per task
-      for (int task = threadIdx.x; task < n2 * n2; task += blockDim.x) {
-        const int ka = task / n2, kb = task % n2;
-        int pa, qa, pb, qb;
-        rr_pair(r, ka, m, pa, qa);
-        rr_pair(r, kb, m, pb, qb);
-        if (ka == kb) {
-          if (pa < n && qa < n) {
-            const double apq = As[pa * ld + qa], tt = js.t[ka];
-            if (tt != 0.0) {
-              As[pa * ld + pa] -= tt * apq;
-              As[qa * ld + qa] += tt * apq;
-              As[pa * ld + qa] = 0.0;
-              As[qa * ld + pa] = 0.0;
-            }
-          }
-          continue;
-        }
-        const double ca = js.c[ka], sa = js.s[ka], cb = js.c[kb], sb = js.s[kb];
-        const bool vpa = pa < n, vqa = qa < n, vpb = pb < n, vqb = qb < n;
-        const double x00 = (vpa && vpb) ? As[pa * ld + pb] : 0.0;
-        const double x01 = (vpa && vqb) ? As[pa * ld + qb] : 0.0;
-        const double x10 = (vqa && vpb) ? As[qa * ld + pb] : 0.0;
-        const double x11 = (vqa && vqb) ? As[qa * ld + qb] : 0.0;
-        // rows: p' = c p - s q, q' = s p + c q
-        const double y00 = ca * x00 - sa * x10, y01 = ca * x01 - sa * x11;
-        const double y10 = sa * x00 + ca * x10, y11 = sa * x01 + ca * x11;
-        // columns
-        if (vpa && vpb) As[pa * ld + pb] = cb * y00 - sb * y01;
-        if (vpa && vqb) As[pa * ld + qb] = sb * y00 + cb * y01;
-        if (vqa && vpb) As[qa * ld + pb] = cb * y10 - sb * y11;
-        if (vqa && vqb) As[qa * ld + qb] = sb * y10 + cb * y11;
-      }
-      // V <- V G: task (row i, pair k)
-      for (int task = threadIdx.x; task < n * n2; task += blockDim.x) {
-        const int i = task / n2, k = task % n2;
+      for (int k = warp; k < n2; k += NW) {
         int p, q;
         rr_pair(r, k, m, p, q);
         if (p >= n || q >= n) continue;
-        const double c = js.c[k], s = js.s[k];
-        if (s == 0.0) continue;
-        double* row = V + (int64_t)i * n;
-        const double vp = row[p], vq = row[q];
-        row[p] = c * vp - s * vq;
-        row[q] = s * vp + c * vq;
+        double* gp = G + (int64_t)p * ldg;
+        double* gq = G + (int64_t)q * ldg;
+        double x[kColRegs], y[kColRegs];
+        double al = 0.0, be = 0.0, ga = 0.0;
+#pragma unroll
+        for (int j = 0; j < kColRegs; ++j) {
+          const int i = lane + 32 * j;
+          x[j] = i < n ? gp[i] : 0.0;
+          y[j] = i < n ? gq[i] : 0.0;
+          al = fma(x[j], x[j], al);
+          be = fma(y[j], y[j], be);
+          ga = fma(x[j], y[j], ga);
+        }
+        al = warp_sum(al);
+        be = warp_sum(be);
+        ga = warp_sum(ga);
+        const double nrm = sqrt(al * be);
+        if (!(fabs(ga) > rot_tol * nrm)) {
+          if (ga != ga) worst = INFINITY;
+          continue;
+        }
+        worst = fmax(worst, fabs(ga) / nrm);
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
+        const double c = 1.0 / sqrt(fma(t, t, 1.0)), s = c * t;
+#pragma unroll
+        for (int j = 0; j < kColRegs; ++j) {
+          const int i = lane + 32 * j;
+          if (i < n) {
+            gp[i] = c * x[j] - s * y[j];
+            gq[i] = s * x[j] + c * y[j];
+          }
+        }
+        double* vp = V + (int64_t)p * ldv;
+        double* vq = V + (int64_t)q * ldv;
+#pragma unroll
+        for (int j = 0; j < kColRegs; ++j) {
+          const int i = lane + 32 * j;
+          x[j] = i < n ? vp[i] : 0.0;
+          y[j] = i < n ? vq[i] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < kColRegs; ++j) {
+          const int i = lane + 32 * j;
+          if (i < n) {
+            vp[i] = c * x[j] - s * y[j];
+            vq[i] = s * x[j] + c * y[j];
+          }
+        }
       }
       __syncthreads();
     }
+    worst = block_max<NT>(worst, red);
+    if (!(worst < INFINITY)) return -1;
+    if (worst < done_tol) return sweep + 1;
   }
   return -1;
+}
+
+// eig[i] = g_i . v_i - mu (one warp per column)
+template <int NT>
+__device__ void block_rayleigh(int n, const double* G, int ldg, const double* V, int ldv,
+                               double mu, double* eig) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = warp; i < n; i += NT / 32) {
+    double s = 0.0;
+    for (int k = lane; k < n; k += 32) s = fma(G[(int64_t)i * ldg + k], V[(int64_t)i * ldv + k], s);
+    s = warp_sum(s);
+    if (lane == 0) eig[i] = s - mu;
+  }
 }
 
 }  // namespace sgb

@@ -58,7 +58,8 @@ def test_batch_rerun_new_coordinates(gpu_ctx, oracle_mod):
     b = sg.Batch(gpu_ctx, mols)
     b.run(1e-6)
     r1 = b.results()
-    moved = [geo.Molecule(m.Z, m.xyz + 0.01) for m in mols]
+    rng = np.random.default_rng(0)  # a random displacement (a uniform shift would not change E)
+    moved = [geo.Molecule(m.Z, m.xyz + rng.normal(0.0, 0.02, m.xyz.shape)) for m in mols]
     b.set_coordinates(np.concatenate([m.xyz.reshape(-1) for m in moved]))
     b.run(1e-6)
     r2 = b.results()
