@@ -121,6 +121,13 @@ int sgb_batch_last_ms(const sgb_batch *b, float *ms);
  * t_end[m] - min(t_begin). */
 int sgb_batch_timestamps(sgb_ctx *ctx, sgb_batch *b, unsigned long long *t_begin,
                          unsigned long long *t_end);
+/* Stage timers (the reference prints per-step Lapack/Pmat/Fmat/Ener times,
+ * scfcalculation.cpp:83-140).  When on, each run records per molecule SGB_STAGE_SLOTS SM-cycle
+ * counters: integrals, Hcore, Fock+energy, warm-start product, Jacobi, eigenvalues+sort,
+ * density, core-core, then counts: Jacobi sweeps, occupied-virtual eigensolves, full ones. */
+#define SGB_STAGE_SLOTS 11
+int sgb_batch_set_profiling(sgb_batch *b, int on);
+int sgb_batch_stage_cycles(sgb_ctx *ctx, sgb_batch *b, unsigned long long *cycles);
 /* Device pointer of the batch's coordinate buffer (natoms_total*3 doubles) for callers that
  * stage inputs themselves. */
 int sgb_batch_device_coordinates(sgb_batch *b, void **dptr);

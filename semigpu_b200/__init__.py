@@ -57,6 +57,8 @@ SIGNATURES = {
     "sgb_batch_device_coordinates": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "sgb_batch_timestamps": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_ulonglong),
                                             ctypes.POINTER(ctypes.c_ulonglong)]),
+    "sgb_batch_set_profiling": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sgb_batch_stage_cycles": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_ulonglong)]),
 }
 
 _lib = None
@@ -259,6 +261,21 @@ class Batch:
         self.ctx.check(lib().sgb_batch_timestamps(self.ctx.h, self.h, tb.ctypes.data_as(P),
                                                   te.ctypes.data_as(P)), "timestamps")
         return tb, te
+
+    STAGES = ("integrals", "hcore", "fock", "warm_gemm", "jacobi", "eigval_sort", "density",
+              "core_core", "sweeps", "bipartite_solves", "full_solves")
+
+    def set_profiling(self, on: bool = True):
+        lib().sgb_batch_set_profiling(self.h, int(on))
+
+    def stage_cycles(self) -> np.ndarray:
+        """(nmol, 11) per-stage SM cycles of the last run, then counts (Jacobi sweeps,
+        occupied-virtual eigensolves, full eigensolves)."""
+        out = np.zeros((self.nmol, len(self.STAGES)), np.uint64)
+        self.ctx.check(lib().sgb_batch_stage_cycles(
+            self.ctx.h, self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong))),
+            "stage_cycles")
+        return out
 
     def device_coordinates(self) -> int:
         p = _VP()

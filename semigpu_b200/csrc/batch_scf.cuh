@@ -3,16 +3,16 @@
 // Molecules are handed out in the order given by `order` (the host sorts by estimated cost,
 // largest first, so the tail of the launch holds the cheap ones).
 //
-// Shared memory holds the eigensolver's working matrix G = (F + mu I) V (odd leading
+// Shared memory holds the eigensolver's working matrix G = F V (odd leading
 // dimension) and, for nao <= 110, the eigenvectors V as well; the per-atom pair densities and a
 // few reduction slots follow.  Hcore, P, F (packed and full) live in global memory
 // (L2-resident at these sizes), as does V for the larger molecules.
 //
 // The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
 // repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
-// max_iter steps.  The eigensolve is a one-sided Jacobi on (F + mu I) V; after the first step
-// it is warm-started from the previous eigenvectors, whose columns the new F barely mixes, so
-// it converges in one or two sweeps.
+// max_iter steps.  The eigensolve is a cyclic Jacobi on V^T F V carried on the columns of V and
+// G = F V; after the first step it is warm-started from the previous eigenvectors, which the
+// new F barely mixes, so it needs few sweeps.
 #pragma once
 #include "scf_block.cuh"
 
@@ -50,6 +50,29 @@ struct BatchArgs {
   int stages;       // STAGE_* bits
   unsigned long long* t_begin;  // optional per-molecule %globaltimer (ns) at start / end
   unsigned long long* t_end;
+  unsigned long long* stage_cycles;  // optional, kStageSlots SM cycles per molecule
+};
+
+// Stage timers (SM clock cycles of the CTA, thread 0, between block-wide barriers), the
+// analogue of the reference's per-step Lapack/Pmat/Fmat/Ener timers
+// (scfcalculation.cpp:83-140).
+enum : int { ST_INTS = 0, ST_HCORE, ST_FOCK, ST_SHIFT_GEMM, ST_JACOBI, ST_EIGVAL_SORT,
+             ST_DENSITY, ST_CORECORE, ST_SWEEPS, ST_BIPARTITE, ST_FULLJAC, kStageSlots };
+
+struct StageClock {
+  unsigned long long* out;
+  long long t;
+  __device__ __forceinline__ void start() { if (out) t = clock64(); }
+  __device__ __forceinline__ void lap(int slot) {
+    if (out) {
+      const long long now = clock64();
+      if (threadIdx.x == 0) out[slot] += (unsigned long long)(now - t);
+      t = now;
+    }
+  }
+  __device__ __forceinline__ void add(int slot, unsigned long long v) {
+    if (out && threadIdx.x == 0) out[slot] += v;
+  }
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -70,6 +93,24 @@ __host__ __device__ inline int smem_ld(int n) { return n | 1; }
 // per launch (mat_doubles); the small arrays follow it.
 constexpr int kVsmemMax = 110;  // 2 * 110 * 111 doubles = 195 KB: G and V both in smem
 
+// Jacobi thresholds, absolute in eV (Fock elements are O(1..100) eV): rotations below
+// kJacobiRotAbs are skipped; sweeps end after one whose largest off-diagonal was below
+// kJacobiDoneAbs, which leaves occupied-virtual couplings of order 1e-14 / gap.
+constexpr double kJacobiRotAbs = 1e-12;
+constexpr double kJacobiDoneAbs = 1e-7;
+
+// The first kFullJacobiSteps eigensolves of an SCF rotate every pair (the occupied set is still
+// moving).  Later ones rotate occupied-virtual pairs only and are accepted when the largest
+// occupied Rayleigh quotient stays kCrossMargin eV below the smallest virtual one (the
+// quotients differ from eigenvalues by the small within-block couplings left unrotated);
+// otherwise a full Jacobi follows, so the occupied set is always the nocc lowest states.
+constexpr int kFullJacobiSteps = 3;
+constexpr double kCrossMargin = 1.0;
+// Occupied-virtual couplings sit across a gap of at least kCrossMargin, where Jacobi converges
+// quadratically: after a sweep whose largest coupling was below kJacobiDoneGapped the next
+// would start below n * 3e-6^2 / 1 eV ~ 1e-9 eV (n <= 160), so no confirmation sweep is run.
+constexpr double kJacobiDoneGapped = 3e-6;
+
 __host__ __device__ inline size_t mat_doubles_for(int n) {
   const size_t ld = (size_t)smem_ld(n);
   return (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
@@ -79,7 +120,7 @@ __host__ __device__ inline size_t extra_doubles(int nmax) {
   return 3 * (size_t)nmax + 8   // wq (<= 2.5 n) + pad
          + (size_t)nmax          // eigenvalues of the last eigensolve
          + 32                    // reductions
-         + (size_t)nmax / 2 + 1; // occupied index list (ints, two per double)
+         + (size_t)nmax + 2;     // occupied and virtual index lists (ints, two per double)
 }
 
 __device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& d) {
@@ -149,7 +190,16 @@ __device__ __forceinline__ int ascending_rank(const double* dval, int n, int i) 
   return rank;
 }
 
-template <int NT>
+// occ <- indices of the nocc smallest dval (in ascending order), vir <- the rest (ascending)
+__device__ inline void split_by_rank(const double* dval, int n, int nocc, int* occ, int* vir) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int rank = ascending_rank(dval, n, i);
+    if (rank < nocc) occ[rank] = i;
+    else vir[rank - nocc] = i;
+  }
+}
+
+template <int NT, int CR>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
   const MolView m = make_view(a, d);
@@ -163,16 +213,23 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   double* dval = wq + 3 * nmax + 8;
   double* red = dval + nmax;
   int* occ = reinterpret_cast<int*>(red + 32);
+  int* vir = occ + nmax + 2;
   double* Ffull = m.T;  // F as a full n x n matrix, global scratch
   if (a.t_begin && threadIdx.x == 0) a.t_begin[mi] = global_ns();
+  StageClock clk{a.stage_cycles ? a.stage_cycles + (int64_t)mi * kStageSlots : nullptr, 0};
+  if (clk.out && threadIdx.x == 0)
+    for (int k = 0; k < kStageSlots; ++k) clk.out[k] = 0;
+  clk.start();
 
   if (a.stages & STAGE_INTS) {
     block_integrals(m);
     __syncthreads();
+    clk.lap(ST_INTS);
   }
   if (a.stages & STAGE_HCORE) {
     block_hcore(m);
     __syncthreads();
+    clk.lap(ST_HCORE);
   }
   double E = 0.0;
   int steps = 0, conv = 0, status = MOL_OK;
@@ -180,29 +237,61 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     block_guess(m);
     __syncthreads();
     E = block_fock_energy<NT>(m, Ffull, n, wq, red);
+    clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     while (!conv && steps < a.max_iter) {
-      // ---- eigensolve of F: one-sided Jacobi on (F + mu I) V, V warm-started ----
-      const double mu = block_shift<NT>(n, Ffull, red);
+      // ---- eigensolve of F: Jacobi on V^T F V through (V, G = F V), V warm-started ----
       if (steps == 0) {
         for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
           const int j = t / n, i = t % n;
           V[(int64_t)j * ldv + i] = i == j ? 1.0 : 0.0;
-          G[(int64_t)j * ld + i] = Ffull[t] + (i == j ? mu : 0.0);
+          G[(int64_t)j * ld + i] = Ffull[t];
         }
       } else {
-        block_shifted_product(n, Ffull, mu, V, ldv, G, ld);
+        block_shifted_product(n, Ffull, 0.0, V, ldv, G, ld);
       }
       __syncthreads();
-      const int sw = block_onesided_jacobi<NT>(n, G, ld, V, ldv, red, 1e-15, 1e-10, 40);
+      clk.lap(ST_SHIFT_GEMM);
+      const int nocc = m.nocc, nvir = n - nocc;
+      int sw;
+      bool full = steps < kFullJacobiSteps || a.sorted_vectors || nocc == 0 || nvir == 0;
+      if (!full) {
+        // occupied / virtual split of the warm-started columns by their Rayleigh quotients
+        block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+        __syncthreads();
+        split_by_rank(dval, n, nocc, occ, vir);
+        __syncthreads();
+        const bool o_small = nocc <= nvir;
+        sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneGapped, 40,
+                                     o_small ? occ : vir, o_small ? nocc : nvir,
+                                     o_small ? vir : occ, o_small ? nvir : nocc);
+        if (sw >= 0) {
+          clk.add(ST_BIPARTITE, 1);
+          // the occupied block must still hold the lowest states (no level crossing)
+          block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+          __syncthreads();
+          double hi = -INFINITY, lo = INFINITY;
+          for (int i = threadIdx.x; i < nocc; i += blockDim.x) hi = fmax(hi, dval[occ[i]]);
+          for (int i = threadIdx.x; i < nvir; i += blockDim.x) lo = fmin(lo, dval[vir[i]]);
+          hi = block_max<NT>(hi, red);
+          lo = -block_max<NT>(-lo, red);
+          full = !(hi + kCrossMargin < lo);
+        }
+      }
+      if (full) {
+        clk.add(ST_FULLJAC, 1);
+        sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
+        if (sw >= 0) {
+          block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+          __syncthreads();
+          split_by_rank(dval, n, nocc, occ, vir);
+        }
+      }
+      clk.lap(ST_JACOBI);
+      clk.add(ST_SWEEPS, (unsigned long long)(sw > 0 ? sw : 0));
       if (sw < 0) { status = MOL_EIG_FAILED; break; }
-      block_rayleigh<NT>(n, G, ld, V, ldv, mu, dval);
       __syncthreads();
-      for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        const int rank = ascending_rank(dval, n, i);
-        if (rank < m.nocc) occ[rank] = i;
-      }
-      __syncthreads();
+      clk.lap(ST_EIGVAL_SORT);
       // ---- density from the occupied vectors, gathered into the G region ----
       for (int t = threadIdx.x; t < n * m.nocc; t += blockDim.x) {
         const int k = t / n, i = t % n;
@@ -211,9 +300,11 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       __syncthreads();
       block_density(n, m.nocc, G, ld, m.P);
       __syncthreads();
+      clk.lap(ST_DENSITY);
       // ---- Fock + energy ----
       const double Eold = E;
       E = block_fock_energy<NT>(m, Ffull, n, wq, red);
+      clk.lap(ST_FOCK);
       ++steps;
       if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride + steps] = E;
       if (E != E) { status = MOL_NAN; break; }
@@ -236,7 +327,11 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     if (threadIdx.x == 0) a.e_el[mi] = E;
   }
   double ecc = 0.0;
-  if (a.stages & STAGE_CC) ecc = block_core_core<NT>(m, red);
+  if (a.stages & STAGE_CC) {
+    clk.start();
+    ecc = block_core_core<NT>(m, red);
+    clk.lap(ST_CORECORE);
+  }
   if (threadIdx.x == 0) {
     if (a.stages & STAGE_SCF) {
       a.e_el[mi] = E;
@@ -250,7 +345,8 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   __syncthreads();
 }
 
-template <int NT>
+// NT threads per CTA; CR column registers per lane in the eigensolver (nao <= 32 * CR).
+template <int NT, int CR>
 __global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
   extern __shared__ double smem[];
   __shared__ int s_next;
@@ -260,7 +356,7 @@ __global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
     const int q = s_next;
     __syncthreads();
     if (q >= a.nmol) break;
-    run_molecule<NT>(a, a.order[q], smem);
+    run_molecule<NT, CR>(a, a.order[q], smem);
   }
 }
 

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -19,8 +20,23 @@ using namespace sgb;
 
 namespace {
 
-constexpr int kThreads = 512;
 constexpr int kSmallNmax = 160;  // largest nao whose n x n FP64 matrix fits one CTA's smem
+
+// Size classes of the batched launch, by nao: (upper bound, eigenvector column registers per
+// lane, default threads per CTA).  The last class holds molecules too large for the in-CTA
+// SCF; only the integral, Hcore, Fock and core-core stages run there.
+struct SizeClass {
+  int nmax, cr, threads;
+};
+constexpr SizeClass kClasses[] = {{64, 2, 512}, {96, 3, 512}, {128, 4, 512}, {160, 5, 512},
+                                  {1 << 30, 2, 512}};
+constexpr int kNumClasses = 5;
+
+int class_of(int nao) {
+  int c = 0;
+  while (nao > kClasses[c].nmax) ++c;
+  return c;
+}
 constexpr size_t kAlign = 256;
 
 __global__ void k_ang_to_bohr(const double* __restrict__ xyz, double* __restrict__ pos,
@@ -41,6 +57,9 @@ struct sgb_ctx {
   size_t smem_optin = 0;
   std::string err;
   sgb_batch* cached = nullptr;  // reused by sgb_run_molecules
+  cudaStream_t aux[kNumClasses] = {};
+  cudaEvent_t joined[kNumClasses] = {};
+  int class_threads[kNumClasses] = {};
 };
 
 struct sgb_batch {
@@ -52,6 +71,7 @@ struct sgb_batch {
   std::vector<int> order;
   std::vector<int> natoms;
   std::vector<int> Z;
+  int class_first[kNumClasses] = {}, class_count[kNumClasses] = {}, class_nmax[kNumClasses] = {};
   char* arena = nullptr;
   size_t bytes = 0;
   MolDesc* d_desc = nullptr;
@@ -68,6 +88,8 @@ struct sgb_batch {
   double *d_eel = nullptr, *d_ecc = nullptr;
   int *d_niter = nullptr, *d_conv = nullptr, *d_status = nullptr;
   unsigned long long *d_tb = nullptr, *d_te = nullptr;
+  unsigned long long* d_stage = nullptr;
+  bool profiling = false;
   double* d_hist = nullptr;
   int hist_stride = 0;
   int64_t n_ints = 0, n_pk = 0, n_sq = 0, n_ao = 0;
@@ -181,23 +203,34 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->natoms_total = atom0;
   b->n_ints = blk0; b->n_pk = pk0; b->n_sq = sq0; b->n_ao = ao0;
   b->hist_stride = hist_stride;
+  // order: grouped by size class, largest estimated cost first within a class
   b->order.resize(nmol);
   for (int m = 0; m < nmol; ++m) b->order[m] = m;
-  std::stable_sort(b->order.begin(), b->order.end(),
-                   [&](int x, int y) { return cost_of(b->desc[x]) > cost_of(b->desc[y]); });
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) {
+    const int cx = class_of(b->desc[x].nao), cy = class_of(b->desc[y].nao);
+    if (cx != cy) return cx > cy;
+    return cost_of(b->desc[x]) > cost_of(b->desc[y]);
+  });
+  for (int q = 0; q < nmol; ++q) {
+    const int c = class_of(b->desc[b->order[q]].nao);
+    if (!b->class_count[c]) b->class_first[c] = q;
+    ++b->class_count[c];
+    b->class_nmax[c] = std::max(b->class_nmax[c], b->desc[b->order[q]].nao);
+  }
 
   // one arena
   const int64_t NA = atom0;
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
   const size_t o_desc = take(sizeof(MolDesc) * nmol), o_order = take(sizeof(int) * nmol),
-               o_counter = take(sizeof(int)), o_slot = take(NA), o_xyz = take(24 * NA),
+               o_counter = take(sizeof(int) * kNumClasses), o_slot = take(NA), o_xyz = take(24 * NA),
                o_pos = take(24 * NA), o_first = take(4 * NA), o_roff = take(8 * NA),
                o_hb = take(4 * NA), o_ints = take(8 * b->n_ints), o_H = take(8 * b->n_pk),
                o_P = take(8 * b->n_pk), o_F = take(8 * b->n_pk), o_V = take(8 * b->n_sq),
                o_T = take(8 * b->n_sq), o_eig = take(8 * b->n_ao), o_eel = take(8 * nmol),
                o_ecc = take(8 * nmol), o_nit = take(4 * nmol), o_conv = take(4 * nmol),
                o_stat = take(4 * nmol), o_tb = take(8 * nmol), o_te = take(8 * nmol),
+               o_stage = take(8 * (size_t)kStageSlots * nmol),
                o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0);
   b->bytes = off;
   if (ctx->budget && ctx->in_use + off > ctx->budget) {
@@ -235,6 +268,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->d_status = (int*)(base + o_stat);
   b->d_tb = (unsigned long long*)(base + o_tb);
   b->d_te = (unsigned long long*)(base + o_te);
+  b->d_stage = (unsigned long long*)(base + o_stage);
   b->d_hist = hist_stride > 0 ? (double*)(base + o_hist) : nullptr;
   cudaStream_t st = ctx->stream;
   auto up = [&](void* dst, const void* src, size_t bytes) {
@@ -262,17 +296,49 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   return SGB_OK;
 }
 
+// One kernel instantiation per (threads per CTA, eigenvector column registers per lane).
+template <int NT, int CR>
+cudaError_t launch_kernel(sgb_ctx* ctx, const BatchArgs& a, size_t smem, cudaStream_t st) {
+  auto* k = k_batch_scf<NT, CR>;
+  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) return cudaErrorInvalidConfiguration;
+  const int grid = std::min(a.nmol, per_sm * ctx->num_sms);
+  k<<<grid, NT, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_class(sgb_ctx* ctx, const BatchArgs& a, int cr, int threads, size_t smem,
+                         cudaStream_t st) {
+  if (threads == 512) {
+    switch (cr) {
+      case 2: return launch_kernel<512, 2>(ctx, a, smem, st);
+      case 3: return launch_kernel<512, 3>(ctx, a, smem, st);
+      case 4: return launch_kernel<512, 4>(ctx, a, smem, st);
+      default: return launch_kernel<512, 5>(ctx, a, smem, st);
+    }
+  }
+  switch (cr) {
+    case 2: return launch_kernel<256, 2>(ctx, a, smem, st);
+    case 3: return launch_kernel<256, 3>(ctx, a, smem, st);
+    case 4: return launch_kernel<256, 4>(ctx, a, smem, st);
+    default: return launch_kernel<256, 5>(ctx, a, smem, st);
+  }
+}
+
+// Runs the requested stages over every molecule: one persistent launch per size class, each on
+// its own stream so the classes share the GPU, joined back into the context stream.
 int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_iter,
                   int sorted_vectors) {
-  const bool needs_smem = stages & (STAGE_SCF | STAGE_FOCK);
-  if (needs_smem && b->nmax > kSmallNmax)
+  const bool scf = stages & STAGE_SCF;
+  if (scf && b->nmax > kSmallNmax)
     return fail(ctx, SGB_E_UNSUPPORTED,
-                "SCF/Fock for nao=%d: the in-shared-memory path takes nao <= %d", b->nmax, kSmallNmax);
+                "SCF for nao=%d: the in-shared-memory path takes nao <= %d", b->nmax, kSmallNmax);
   BatchArgs a;
-  a.nmol = b->nmol;
   a.mols = b->d_desc;
-  a.order = b->d_order;
-  a.counter = b->d_counter;
   a.slot = b->d_slot;
   a.pos = b->d_pos;
   a.first = b->d_first;
@@ -286,30 +352,39 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.hist = b->d_hist; a.hist_stride = b->hist_stride;
   a.tol = tol;
   a.max_iter = std::min(max_iter, b->hist_stride > 0 ? b->hist_stride - 1 : max_iter);
-  // stages without the SCF matrix still use the reduction slots of the shared layout
-  a.nmax = needs_smem ? std::max(1, b->nmax) : 1;
   a.sorted_vectors = sorted_vectors;
   a.stages = stages;
   a.t_begin = b->d_tb;
   a.t_end = b->d_te;
-  a.mat_doubles = 0;
-  if (needs_smem)
-    for (const MolDesc& d : b->desc) a.mat_doubles = std::max(a.mat_doubles, mat_doubles_for(d.nao));
-  const size_t smem = (a.mat_doubles + extra_doubles(a.nmax)) * sizeof(double);
+  a.stage_cycles = b->profiling ? b->d_stage : nullptr;
   cudaStream_t st = ctx->stream;
-  CUDA_TRY(ctx, cudaFuncSetAttribute(k_batch_scf<kThreads>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_scf<kThreads>,
-                                                              kThreads, smem));
-  if (per_sm < 1) return fail(ctx, SGB_E_CUDA, "kernel does not fit an SM (smem %zu)", smem);
-  const int grid = std::min(b->nmol, per_sm * ctx->num_sms);
-  CUDA_TRY(ctx, cudaMemsetAsync(b->d_counter, 0, sizeof(int), st));
+  CUDA_TRY(ctx, cudaMemsetAsync(b->d_counter, 0, sizeof(int) * kNumClasses, st));
   CUDA_TRY(ctx, cudaEventRecord(b->ev0, st));
-  k_batch_scf<kThreads><<<grid, kThreads, smem, st>>>(a);
-  CUDA_TRY(ctx, cudaGetLastError());
+  int used = 0;
+  for (int c = 0; c < kNumClasses; ++c) {
+    const int cnt = b->class_count[c];
+    if (!cnt) continue;
+    BatchArgs ac = a;
+    ac.nmol = cnt;
+    ac.order = b->d_order + b->class_first[c];
+    ac.counter = b->d_counter + c;
+    ac.nmax = std::max(1, b->class_nmax[c]);
+    ac.mat_doubles = 0;
+    if (scf)
+      for (int q = 0; q < cnt; ++q)
+        ac.mat_doubles = std::max(ac.mat_doubles,
+                                  mat_doubles_for(b->desc[b->order[b->class_first[c] + q]].nao));
+    const size_t smem = (ac.mat_doubles + extra_doubles(ac.nmax)) * sizeof(double);
+    cudaStream_t cs = ctx->aux[c];
+    CUDA_TRY(ctx, cudaStreamWaitEvent(cs, b->ev0, 0));
+    cudaError_t e = launch_class(ctx, ac, kClasses[c].cr, ctx->class_threads[c], smem, cs);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "k_batch_scf launch");
+    CUDA_TRY(ctx, cudaEventRecord(ctx->joined[c], cs));
+    CUDA_TRY(ctx, cudaStreamWaitEvent(st, ctx->joined[c], 0));
+    ++used;
+  }
   CUDA_TRY(ctx, cudaEventRecord(b->ev1, st));
-  return SGB_OK;
+  return used ? SGB_OK : fail(ctx, SGB_E_ARG, "empty batch");
 }
 
 }  // namespace
@@ -355,6 +430,23 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   c->smem_optin = optin;
+  for (int k = 0; k < kNumClasses; ++k) {
+    c->class_threads[k] = kClasses[k].threads;
+    if (cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->joined[k], cudaEventDisableTiming) != cudaSuccess) {
+      sgb_ctx_destroy(c);
+      return SGB_E_CUDA;
+    }
+  }
+  if (const char* env = getenv("SGB_CLASS_THREADS")) {  // e.g. "256,512,512,512"
+    int k = 0;
+    for (const char* p = env; *p && k < kNumClasses; ++k) {
+      const int t = atoi(p);
+      if (t == 256 || t == 512) c->class_threads[k] = t;
+      while (*p && *p != ',') ++p;
+      if (*p == ',') ++p;
+    }
+  }
   *out = c;
   return SGB_OK;
 }
@@ -363,6 +455,10 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
   if (!ctx) return SGB_E_ARG;
   cudaSetDevice(ctx->device);
   free_batch(ctx->cached);
+  for (int k = 0; k < kNumClasses; ++k) {
+    if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
+    if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return SGB_OK;
@@ -550,6 +646,20 @@ int sgb_batch_timestamps(sgb_ctx* ctx, sgb_batch* b, unsigned long long* t_begin
   const size_t n = (size_t)b->nmol;
   if (t_begin) CUDA_TRY(ctx, cudaMemcpyAsync(t_begin, b->d_tb, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
   if (t_end) CUDA_TRY(ctx, cudaMemcpyAsync(t_end, b->d_te, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  return sgb_ctx_synchronize(ctx);
+}
+
+int sgb_batch_set_profiling(sgb_batch* b, int on) {
+  if (!b) return SGB_E_ARG;
+  b->profiling = on != 0;
+  return SGB_OK;
+}
+
+int sgb_batch_stage_cycles(sgb_ctx* ctx, sgb_batch* b, unsigned long long* cycles) {
+  if (!ctx || !b || !cycles) return SGB_E_ARG;
+  if (!b->profiling) return fail(ctx, SGB_E_STATE, "stage timers are off (sgb_batch_set_profiling)");
+  CUDA_TRY(ctx, cudaMemcpyAsync(cycles, b->d_stage, 8 * (size_t)kStageSlots * b->nmol,
+                                cudaMemcpyDeviceToHost, ctx->stream));
   return sgb_ctx_synchronize(ctx);
 }
 

@@ -326,7 +326,7 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   if (l == 0) red[w] = v;
   __syncthreads();
   if (w == 0) {
-    v = (l < NT / 32) ? red[l] : 0.0;
+    v = (l < NT / 32) ? red[l] : -INFINITY;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
     if (l == 0) red[0] = v;
@@ -396,18 +396,21 @@ __device__ inline void block_shifted_product(int n, const double* F, double mu, 
 }
 
 // ------------------------------------------------------------------------------------------
-// One-sided (Hestenes) cyclic Jacobi.  G = (F + mu I) V0 with V0 orthogonal; rotations from
-// the right orthogonalise the columns of G and are accumulated into V (both column-major).
-// With F + mu I positive semi-definite the converged V holds eigenvectors of F and
-// g_i . v_i - mu its eigenvalues.  A rotation touches two columns only, so one warp owns one
-// column pair of a round (columns held in registers, n <= 32 * kColRegs); rounds follow the
-// round-robin ordering (ne = n rounded up to even, m = ne - 1: round r pairs m with r and
-// (r + k) % m with (r - k) % m; an index >= n is a dummy).  A rotation is skipped when
-// |g_p.g_q| <= rot_tol sqrt(|g_p|^2 |g_q|^2); sweeps stop after one whose largest measured
-// off-diagonal cosine was below done_tol (the next would start from its square).  Returns the
-// sweep count, or -1 if max_sweeps ran out or a non-finite value appeared.
-constexpr int kColRegs = 5;  // n <= 160
-
+// Cyclic Jacobi on A = V^T F V carried out on columns only.  The CTA keeps V (orthogonal,
+// column-major) and G = F V; a two-sided rotation J of A in the (p, q) plane is
+// A <- J^T A J, which is exactly V <- V J together with G <- G J.  Its angle needs
+// A_pp = v_p.g_p, A_qq = v_q.g_q and A_pq = (v_p.g_q + g_p.v_q) / 2 -- four dot products of the
+// pair's own columns -- so one warp owns one column pair per round (columns in registers,
+// n <= 32 * CR) and a round needs one barrier.  Convergence is that of two-sided Jacobi on
+// F (no spectral shift).  Pairs follow the round-robin ordering (ne = n rounded up to even,
+// m = ne - 1: round r pairs m with r and (r + k) % m with (r - k) % m; an index >= n is a
+// dummy).  CR doubles per lane hold one column, so n <= 32 * CR.
+//
+// The rotation's tangent is computed in FP32 (an approximate angle only leaves a residual the
+// next sweep removes); c = rsqrt(1 + t^2) and s = c t are FP64, so every applied rotation is
+// orthogonal to rounding.  A pair is skipped when |A_pq| <= rot_abs; sweeps stop after one
+// whose largest |A_pq| was below done_abs (the next would start from about its square over the
+// gap).  Returns the sweep count, or -1 (max_sweeps exhausted or a non-finite value).
 __device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
   if (k == 0) { p = m; q = r; }
   else {
@@ -416,66 +419,85 @@ __device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
   }
 }
 
-template <int NT>
-__device__ int block_onesided_jacobi(int n, double* G, int ldg, double* V, int ldv, double* red,
-                                     double rot_tol, double done_tol, int max_sweeps) {
+//
+// Bipartite mode (grp_a != nullptr): only pairs between the index sets grp_a (na entries) and
+// grp_b (nb entries, na <= nb) are rotated -- round r pairs grp_a[k] with grp_b[(k + r) % nb],
+// nb rounds per sweep.  The SCF uses it with the occupied and virtual columns: the density
+// matrix only depends on the occupied subspace, which these rotations alone decide.
+template <int NT, int CR>
+__device__ int block_jacobi_fv(int n, double* G, int ldg, double* V, int ldv, double* red,
+                               double rot_abs, double done_abs, int max_sweeps,
+                               const int* grp_a = nullptr, int na = 0, const int* grp_b = nullptr,
+                               int nb = 0) {
   const int ne = n + (n & 1), m = ne - 1, n2 = ne / 2;
+  const bool bip = grp_a != nullptr;
+  const int rounds = bip ? nb : m, per_round = bip ? na : n2;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   constexpr int NW = NT / 32;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double worst = 0.0;
-    for (int r = 0; r < m; ++r) {
-      for (int k = warp; k < n2; k += NW) {
+    for (int r = 0; r < rounds; ++r) {
+      for (int k = warp; k < per_round; k += NW) {
         int p, q;
-        rr_pair(r, k, m, p, q);
-        if (p >= n || q >= n) continue;
+        if (bip) {
+          p = grp_a[k];
+          int j = k + r;
+          if (j >= nb) j -= nb;
+          q = grp_b[j];
+        } else {
+          rr_pair(r, k, m, p, q);
+          if (p >= n || q >= n) continue;
+        }
         double* gp = G + (int64_t)p * ldg;
         double* gq = G + (int64_t)q * ldg;
-        double x[kColRegs], y[kColRegs];
-        double al = 0.0, be = 0.0, ga = 0.0;
-#pragma unroll
-        for (int j = 0; j < kColRegs; ++j) {
-          const int i = lane + 32 * j;
-          x[j] = i < n ? gp[i] : 0.0;
-          y[j] = i < n ? gq[i] : 0.0;
-          al = fma(x[j], x[j], al);
-          be = fma(y[j], y[j], be);
-          ga = fma(x[j], y[j], ga);
-        }
-        al = warp_sum(al);
-        be = warp_sum(be);
-        ga = warp_sum(ga);
-        const double nrm = sqrt(al * be);
-        if (!(fabs(ga) > rot_tol * nrm)) {
-          if (ga != ga) worst = INFINITY;
-          continue;
-        }
-        worst = fmax(worst, fabs(ga) / nrm);
-        const double zeta = (be - al) / (2.0 * ga);
-        const double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(fma(zeta, zeta, 1.0)));
-        const double c = 1.0 / sqrt(fma(t, t, 1.0)), s = c * t;
-#pragma unroll
-        for (int j = 0; j < kColRegs; ++j) {
-          const int i = lane + 32 * j;
-          if (i < n) {
-            gp[i] = c * x[j] - s * y[j];
-            gq[i] = s * x[j] + c * y[j];
-          }
-        }
         double* vp = V + (int64_t)p * ldv;
         double* vq = V + (int64_t)q * ldv;
+        double xg[CR], yg[CR], xv[CR], yv[CR];
+        double app = 0.0, aqq = 0.0, apq = 0.0, aqp = 0.0;
 #pragma unroll
-        for (int j = 0; j < kColRegs; ++j) {
+        for (int j = 0; j < CR; ++j) {
           const int i = lane + 32 * j;
-          x[j] = i < n ? vp[i] : 0.0;
-          y[j] = i < n ? vq[i] : 0.0;
+          const bool in = i < n;
+          xg[j] = in ? gp[i] : 0.0;
+          yg[j] = in ? gq[i] : 0.0;
+          xv[j] = in ? vp[i] : 0.0;
+          yv[j] = in ? vq[i] : 0.0;
         }
 #pragma unroll
-        for (int j = 0; j < kColRegs; ++j) {
+        for (int j = 0; j < CR; ++j) {
+          app = fma(xv[j], xg[j], app);
+          aqq = fma(yv[j], yg[j], aqq);
+          apq = fma(xv[j], yg[j], apq);
+          aqp = fma(xg[j], yv[j], aqp);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          app += __shfl_xor_sync(0xffffffffu, app, o);
+          aqq += __shfl_xor_sync(0xffffffffu, aqq, o);
+          apq += __shfl_xor_sync(0xffffffffu, apq, o);
+          aqp += __shfl_xor_sync(0xffffffffu, aqp, o);
+        }
+        const double a_pq = 0.5 * (apq + aqp);
+        if (!(fabs(a_pq) > rot_abs)) {
+          if (a_pq != a_pq) worst = INFINITY;
+          continue;
+        }
+        worst = fmax(worst, fabs(a_pq));
+        // tan of the angle zeroing A_pq: t = sgn(den) num / (|den| + hypot(den, num)),
+        // num = 2 A_pq, den = A_qq - A_pp (the smaller of the two roots)
+        const float num = (float)(2.0 * a_pq), den = (float)(aqq - app);
+        float tf = num / (fabsf(den) + hypotf(den, num));
+        if (den < 0.0f) tf = -tf;
+        const double t = (double)tf;
+        const double c = rsqrt(fma(t, t, 1.0)), s = c * t;
+#pragma unroll
+        for (int j = 0; j < CR; ++j) {
           const int i = lane + 32 * j;
           if (i < n) {
-            vp[i] = c * x[j] - s * y[j];
-            vq[i] = s * x[j] + c * y[j];
+            gp[i] = c * xg[j] - s * yg[j];
+            gq[i] = s * xg[j] + c * yg[j];
+            vp[i] = c * xv[j] - s * yv[j];
+            vq[i] = s * xv[j] + c * yv[j];
           }
         }
       }
@@ -483,7 +505,7 @@ __device__ int block_onesided_jacobi(int n, double* G, int ldg, double* V, int l
     }
     worst = block_max<NT>(worst, red);
     if (!(worst < INFINITY)) return -1;
-    if (worst < done_tol) return sweep + 1;
+    if (worst < done_abs) return sweep + 1;
   }
   return -1;
 }
