@@ -72,6 +72,13 @@ size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
  * natoms*3 Cartesian coordinates in Angstrom. */
 int sgb_mol_create(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, sgb_mol **out);
 int sgb_mol_destroy(sgb_mol *mol);
+/* Execution path of the stage calls: AUTO picks one CTA per molecule with its SCF matrices in
+ * shared memory for nao <= 160 and the grid-wide kernels (host-driven SCF loop, cooperative
+ * Jacobi) above that; CTA / GRID force one (CTA refuses SCF above nao 160). */
+#define SGB_PATH_AUTO 0
+#define SGB_PATH_CTA 1
+#define SGB_PATH_GRID 2
+int sgb_mol_set_path(sgb_mol *mol, int path);
 /* nao (ListAtomicOrbitals::size), nocc (DensityMatrix::NumberOfElectrons/2), integral
  * doubles. */
 int sgb_mol_info(const sgb_mol *mol, int *natoms, int *nao, int *nocc, long long *nblocks);

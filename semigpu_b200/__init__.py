@@ -24,6 +24,7 @@ LIB_PATH = os.path.join(HERE, "libsemigpu_b200.so")
 OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN = (
     0, -1, -2, -3, -4, -5, -6, 1, 2)
 BLOCKS, HCORE, FOCK, DENSITY, EIGVAL, EIGVEC = range(6)
+PATH_AUTO, PATH_CTA, PATH_GRID = range(3)
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -40,6 +41,7 @@ SIGNATURES = {
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
     "sgb_mol_destroy": (ctypes.c_int, [_VP]),
     "sgb_mol_info": (ctypes.c_int, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
+    "sgb_mol_set_path": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_two_center": (ctypes.c_int, [_VP, _VP]),
     "sgb_hcore": (ctypes.c_int, [_VP, _VP]),
     "sgb_scf": (ctypes.c_int, [_VP, _VP, ctypes.c_double, ctypes.c_int, _VP, _D]),
@@ -157,6 +159,10 @@ class Molecule:
     @classmethod
     def from_geometry(cls, ctx: Context, mol: geometry.Molecule) -> "Molecule":
         return cls(ctx, mol.Z, mol.xyz)
+
+    def set_path(self, path: int):
+        """PATH_AUTO, PATH_CTA (one CTA per molecule, nao <= 160) or PATH_GRID (whole GPU)."""
+        self.ctx.check(lib().sgb_mol_set_path(self.h, path), "sgb_mol_set_path")
 
     def two_center(self):
         self.ctx.check(lib().sgb_two_center(self.ctx.h, self.h), "sgb_two_center")

@@ -13,6 +13,7 @@
 
 #include "../../include/semigpu_b200.h"
 #include "batch_scf.cuh"
+#include "grid_scf.cuh"
 #include "layout.h"
 #include "mndo_tables.cuh"
 
@@ -97,10 +98,24 @@ struct sgb_batch {
   float last_ms = 0.f;
 };
 
+// Device workspace of the grid-wide path (allocated on first use).
+struct GridWork {
+  char* arena = nullptr;
+  size_t bytes = 0;
+  double *G = nullptr, *Fprev = nullptr, *wq = nullptr, *dval = nullptr, *partial = nullptr;
+  double* scalars = nullptr;  // [0] E_el, [1] E_cc
+  int *occ = nullptr, *vir = nullptr, *flag = nullptr, *result = nullptr;
+  unsigned long long* worst = nullptr;
+  unsigned* bar = nullptr;  // count, generation
+  int* err = nullptr;
+};
+
 struct sgb_mol {
   sgb_ctx* ctx = nullptr;
   sgb_batch* b = nullptr;
   bool ints_done = false, hcore_done = false, scf_done = false;
+  int path = SGB_PATH_AUTO;
+  GridWork gw;
 };
 
 namespace {
@@ -387,6 +402,199 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   return used ? SGB_OK : fail(ctx, SGB_E_ARG, "empty batch");
 }
 
+// ------------------------------------------------------------------------------------------
+// Grid-wide path for one molecule
+
+constexpr int kGridThreads = 256;
+constexpr int kPartialMax = 4096;
+constexpr int kMaxSweeps = 60;
+
+bool use_grid(const sgb_mol* mol) {
+  if (mol->path == SGB_PATH_GRID) return true;
+  if (mol->path == SGB_PATH_CTA) return false;
+  return mol->b->desc[0].nao > kSmallNmax;
+}
+
+MolView mol_view(const sgb_batch* b) {
+  const MolDesc& d = b->desc[0];
+  MolView v;
+  v.natoms = d.natoms; v.nao = d.nao; v.nocc = d.nocc;
+  v.slot = b->d_slot; v.pos = b->d_pos; v.first = b->d_first; v.row_off = b->d_row_off;
+  v.hb = b->d_hb; v.ints = b->d_ints; v.H = b->d_H; v.P = b->d_P; v.F = b->d_F;
+  v.V = b->d_V; v.T = b->d_T; v.eig = b->d_eig;
+  return v;
+}
+
+int grid_blocks(const sgb_ctx* ctx, int64_t tasks) {
+  const int64_t want = (tasks + kGridThreads - 1) / kGridThreads;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kPartialMax, 8LL * ctx->num_sms)));
+}
+
+int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
+  GridWork& w = mol->gw;
+  if (w.arena) return SGB_OK;
+  const int64_t n = mol->b->desc[0].nao;
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
+  const size_t oG = take(8 * n * n), oFp = take(8 * n * n), owq = take(8 * (3 * n + 8)),
+               odv = take(8 * n), opart = take(8 * kPartialMax), osc = take(8 * 4),
+               oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
+               owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
+  if (ctx->budget && ctx->in_use + off > ctx->budget)
+    return fail(ctx, SGB_E_NOMEM, "grid workspace needs %zu bytes over the budget", off);
+  cudaError_t e = cudaMalloc(&w.arena, off);
+  if (e != cudaSuccess) return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
+  ctx->in_use += off;
+  w.bytes = off;
+  char* b = w.arena;
+  w.G = (double*)(b + oG); w.Fprev = (double*)(b + oFp); w.wq = (double*)(b + owq);
+  w.dval = (double*)(b + odv); w.partial = (double*)(b + opart); w.scalars = (double*)(b + osc);
+  w.occ = (int*)(b + oocc); w.vir = (int*)(b + ovir); w.flag = (int*)(b + oflag);
+  w.result = (int*)(b + ores); w.worst = (unsigned long long*)(b + owst);
+  w.bar = (unsigned*)(b + obar); w.err = (int*)(b + oerr);
+  return SGB_OK;
+}
+
+void free_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
+  if (mol->gw.arena) {
+    cudaFree(mol->gw.arena);
+    if (ctx) ctx->in_use -= mol->gw.bytes;
+    mol->gw = GridWork();
+  }
+}
+
+// F (packed + full into T) and E_el into scalars[0]
+int grid_fock(sgb_ctx* ctx, sgb_mol* mol, bool full_matrix) {
+  const MolView v = mol_view(mol->b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  k_grid_pair_density<<<grid_blocks(ctx, (int64_t)v.natoms * 10), kGridThreads, 0, st>>>(v, w.wq);
+  const int nb = grid_blocks(ctx, (int64_t)v.natoms * 10 + tri(v.natoms));
+  k_grid_fock<<<nb, kGridThreads, 0, st>>>(v, w.wq, full_matrix ? v.T : nullptr, w.partial);
+  k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, w.scalars);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return SGB_OK;
+}
+
+// One cooperative Jacobi launch; returns sweeps (>0), -1 no convergence, -2 barrier timeout.
+int grid_jacobi(sgb_ctx* ctx, sgb_mol* mol, const int* ga, int na, const int* gb, int nb,
+                double done_abs, int* sweeps) {
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = mol->b->desc[0].nao;
+  CUDA_TRY(ctx, cudaMemsetAsync(w.worst, 0, 8 * kMaxSweeps, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.bar, 0, 8, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.err, 0, 4, st));
+  GridJacobiArgs a;
+  a.n = n; a.G = w.G; a.V = mol->b->d_V;
+  a.grp_a = ga; a.na = na; a.grp_b = gb; a.nb = nb;
+  a.rot_abs = kJacobiRotAbs; a.done_abs = done_abs; a.max_sweeps = kMaxSweeps;
+  a.worst = w.worst; a.result = w.result; a.bar = GridBarrier{w.bar, w.bar + 1, w.err};
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_jacobi, kGridThreads, 0));
+  const int pairs = ga ? na : (n + 1) / 2;
+  const int blocks = std::max(1, std::min(per_sm * ctx->num_sms, (pairs * 32 + kGridThreads - 1) / kGridThreads));
+  void* args[] = {&a};
+  CUDA_TRY(ctx, cudaLaunchCooperativeKernel((void*)k_grid_jacobi, blocks, kGridThreads, args, 0, st));
+  int r = 0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&r, w.result, 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  *sweeps = r;
+  return SGB_OK;
+}
+
+int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result* res,
+             double* energies) {
+  int rc = ensure_grid_work(ctx, mol);
+  if (rc) return rc;
+  sgb_batch* b = mol->b;
+  const MolView v = mol_view(b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = v.nao, nocc = v.nocc, nvir = n - nocc;
+  const int64_t nn = (int64_t)n * n;
+  k_grid_guess<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(v);
+  k_grid_guess_diag<<<grid_blocks(ctx, v.natoms), kGridThreads, 0, st>>>(v);
+  if ((rc = grid_fock(ctx, mol, true))) return rc;
+  double E = 0.0;
+  CUDA_TRY(ctx, cudaMemcpyAsync(&E, w.scalars, 8, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  std::vector<double> hist(1, E);
+  int steps = 0, conv = 0, status = SGB_OK;
+  const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
+  while (!conv && steps < max_iter) {
+    if (steps == 0)
+      k_grid_identity<<<grid_blocks(ctx, nn), kGridThreads, 0, st>>>(n, b->d_V, w.G, v.T);
+    else
+      k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, v.T, b->d_V, w.G);
+    CUDA_TRY(ctx, cudaGetLastError());
+    bool full = steps < kFullJacobiSteps || nocc == 0 || nvir == 0;
+    int sw = 0;
+    if (!full) {
+      k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+      k_grid_split<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, nocc, w.dval, w.occ, w.vir);
+      const bool o_small = nocc <= nvir;
+      if ((rc = grid_jacobi(ctx, mol, o_small ? w.occ : w.vir, o_small ? nocc : nvir,
+                            o_small ? w.vir : w.occ, o_small ? nvir : nocc, kJacobiDoneGapped, &sw)))
+        return rc;
+      if (sw > 0) {
+        k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+        k_grid_crossing<<<1, 256, 0, st>>>(nocc, nvir, w.dval, w.occ, w.vir, kCrossMargin, w.flag);
+        int cross = 0;
+        CUDA_TRY(ctx, cudaMemcpyAsync(&cross, w.flag, 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(ctx, cudaStreamSynchronize(st));
+        full = cross != 0;
+      }
+    }
+    if (full) {
+      if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
+      if (sw > 0) {
+        k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+        k_grid_split<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, nocc, w.dval, w.occ, w.vir);
+      }
+    }
+    if (sw == -2) return fail(ctx, SGB_E_CUDA, "grid barrier timed out in the Jacobi eigensolver");
+    if (sw < 0) { status = SGB_E_EIG; break; }
+    if (nocc > 0) {
+      const int tiles = (n + 3) / 4;
+      k_grid_density<<<grid_blocks(ctx, (int64_t)tiles * (tiles + 1) / 2), kGridThreads, 0, st>>>(
+          n, nocc, b->d_V, w.occ, v.P);
+    } else {
+      CUDA_TRY(ctx, cudaMemsetAsync(v.P, 0, 8 * tri(n), st));
+    }
+    // keep the F this eigensolve diagonalised: the final eigenpairs are reported for it
+    CUDA_TRY(ctx, cudaMemcpyAsync(w.Fprev, v.T, 8 * nn, cudaMemcpyDeviceToDevice, st));
+    if ((rc = grid_fock(ctx, mol, true))) return rc;
+    const double Eold = E;
+    CUDA_TRY(ctx, cudaMemcpyAsync(&E, w.scalars, 8, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    ++steps;
+    hist.push_back(E);
+    if (E != E) { status = SGB_E_NAN; break; }
+    conv = fabs(Eold - E) < tol;
+  }
+  // eigenpairs of the last eigensolve's F, fully diagonalised (the loop may have rotated only
+  // occupied-virtual pairs), sorted ascending into eig / T
+  if (steps > 0 && status == SGB_OK) {
+    k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, w.Fprev, b->d_V, w.G);
+    int sw = 0;
+    if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
+    if (sw < 0) status = SGB_E_EIG;
+    k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+    k_grid_sorted_output<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, w.dval, b->d_V, v.eig, v.T);
+    CUDA_TRY(ctx, cudaGetLastError());
+  }
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (energies) std::copy(hist.begin(), hist.end(), energies);
+  if (res) {
+    res->e_el = E;
+    res->n_iter = steps;
+    res->converged = conv;
+    res->status = status;
+  }
+  return status;
+}
+
 }  // namespace
 
 // ============================================================================================
@@ -486,8 +694,15 @@ int sgb_mol_create(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, sg
 
 int sgb_mol_destroy(sgb_mol* mol) {
   if (!mol) return SGB_E_ARG;
+  free_grid_work(mol->ctx, mol);
   free_batch(mol->b);
   delete mol;
+  return SGB_OK;
+}
+
+int sgb_mol_set_path(sgb_mol* mol, int path) {
+  if (!mol || path < SGB_PATH_AUTO || path > SGB_PATH_GRID) return SGB_E_ARG;
+  mol->path = path;
   return SGB_OK;
 }
 
@@ -503,8 +718,14 @@ int sgb_mol_info(const sgb_mol* mol, int* natoms, int* nao, int* nocc, long long
 
 int sgb_two_center(sgb_ctx* ctx, sgb_mol* mol) {
   if (!ctx || !mol) return SGB_E_ARG;
-  int rc = launch_stages(ctx, mol->b, STAGE_INTS, 0.0, 0, 0);
-  if (rc) return rc;
+  if (use_grid(mol)) {
+    const MolView v = mol_view(mol->b);
+    k_grid_integrals<<<grid_blocks(ctx, tri(v.natoms)), kGridThreads, 0, ctx->stream>>>(v);
+    CUDA_TRY(ctx, cudaGetLastError());
+  } else {
+    int rc = launch_stages(ctx, mol->b, STAGE_INTS, 0.0, 0, 0);
+    if (rc) return rc;
+  }
   mol->ints_done = true;
   mol->hcore_done = mol->scf_done = false;
   return sgb_ctx_synchronize(ctx);
@@ -513,8 +734,15 @@ int sgb_two_center(sgb_ctx* ctx, sgb_mol* mol) {
 int sgb_hcore(sgb_ctx* ctx, sgb_mol* mol) {
   if (!ctx || !mol) return SGB_E_ARG;
   if (!mol->ints_done) return fail(ctx, SGB_E_STATE, "Hcore needs the two-center integrals");
-  int rc = launch_stages(ctx, mol->b, STAGE_HCORE, 0.0, 0, 0);
-  if (rc) return rc;
+  if (use_grid(mol)) {
+    const MolView v = mol_view(mol->b);
+    k_grid_hcore<<<grid_blocks(ctx, (int64_t)v.natoms * 10 + tri(v.natoms)), kGridThreads, 0,
+                   ctx->stream>>>(v);
+    CUDA_TRY(ctx, cudaGetLastError());
+  } else {
+    int rc = launch_stages(ctx, mol->b, STAGE_HCORE, 0.0, 0, 0);
+    if (rc) return rc;
+  }
   mol->hcore_done = true;
   return sgb_ctx_synchronize(ctx);
 }
@@ -525,6 +753,12 @@ int sgb_scf(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result
   if (!mol->hcore_done) return fail(ctx, SGB_E_STATE, "SCF needs Hcore");
   if (max_iter > mol->b->hist_stride - 1)
     return fail(ctx, SGB_E_ARG, "max_iter %d above %d", max_iter, mol->b->hist_stride - 1);
+  if (use_grid(mol)) {
+    const int st = scf_grid(ctx, mol, tol, max_iter, res, energies);
+    if (st < 0) return st;
+    mol->scf_done = true;
+    return st;
+  }
   int rc = launch_stages(ctx, mol->b, STAGE_SCF, tol, max_iter, 1);
   if (rc) return rc;
   sgb_batch* b = mol->b;
@@ -550,6 +784,17 @@ int sgb_scf(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result
 int sgb_core_core(sgb_ctx* ctx, sgb_mol* mol, double* e_cc) {
   if (!ctx || !mol || !e_cc) return SGB_E_ARG;
   if (!mol->ints_done) return fail(ctx, SGB_E_STATE, "core-core needs the two-center integrals");
+  if (use_grid(mol)) {
+    int rc = ensure_grid_work(ctx, mol);
+    if (rc) return rc;
+    const MolView v = mol_view(mol->b);
+    const int nb = grid_blocks(ctx, tri(v.natoms));
+    k_grid_core_core<<<nb, kGridThreads, 0, ctx->stream>>>(v, mol->gw.partial);
+    k_reduce_sum<<<1, 256, 0, ctx->stream>>>(mol->gw.partial, nb, mol->gw.scalars + 1);
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaMemcpyAsync(e_cc, mol->gw.scalars + 1, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    return sgb_ctx_synchronize(ctx);
+  }
   int rc = launch_stages(ctx, mol->b, STAGE_CC, 0.0, 0, 0);
   if (rc) return rc;
   CUDA_TRY(ctx, cudaMemcpyAsync(e_cc, mol->b->d_ecc, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -562,10 +807,18 @@ int sgb_fock(sgb_ctx* ctx, sgb_mol* mol, const double* P, double* F, double* e_e
   sgb_batch* b = mol->b;
   const size_t np = (size_t)tri(b->desc[0].nao);
   CUDA_TRY(ctx, cudaMemcpyAsync(b->d_P, P, 8 * np, cudaMemcpyHostToDevice, ctx->stream));
-  int rc = launch_stages(ctx, b, STAGE_FOCK, 0.0, 0, 0);
-  if (rc) return rc;
+  const double* e_src = b->d_eel;
+  if (use_grid(mol)) {
+    int rc = ensure_grid_work(ctx, mol);
+    if (!rc) rc = grid_fock(ctx, mol, false);
+    if (rc) return rc;
+    e_src = mol->gw.scalars;
+  } else {
+    int rc = launch_stages(ctx, b, STAGE_FOCK, 0.0, 0, 0);
+    if (rc) return rc;
+  }
   if (F) CUDA_TRY(ctx, cudaMemcpyAsync(F, b->d_F, 8 * np, cudaMemcpyDeviceToHost, ctx->stream));
-  if (e_el) CUDA_TRY(ctx, cudaMemcpyAsync(e_el, b->d_eel, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  if (e_el) CUDA_TRY(ctx, cudaMemcpyAsync(e_el, e_src, 8, cudaMemcpyDeviceToHost, ctx->stream));
   return sgb_ctx_synchronize(ctx);
 }
 

@@ -171,106 +171,119 @@ __device__ inline void block_hcore(const MolView& m) {
 
 // ------------------------------------------------------------------------------------------
 // Fock build + electronic energy.  Writes F packed to global memory and, when Fs != nullptr,
-// the full symmetric F (leading dimension ld).  Returns E_el in every thread.
+// the full symmetric F (leading dimension ld); the CTA version returns E_el in every thread.
 //
-// wq: shared scratch of 10 * nheavy + nlight doubles: the pair densities of each atom,
+// wq: scratch of 10 * nheavy + nlight doubles: the pair densities of each atom,
 //     w_C[q] = P_{lam sig} (x2 when lam != sig) for pair q = (lam, sig) of atom C.
 __device__ __forceinline__ int wq_offset(const MolView& m, int A) { return 9 * m.hb[A] + A; }
+
+// Per-task pieces (used by the CTA path below and by the grid-wide kernels).
+
+// w_C[q] for task t = (C, q)
+__device__ __forceinline__ void pair_density_task(const MolView& m, double* wq, int t) {
+  const int C = t / 10, q = t % 10;
+  const int s = m.slot[C];
+  if (s == 0 && q) return;
+  const int a = pair_first(q), b = pair_second(q), f = m.first[C];
+  const double p = m.P[tri(f + b) + f + a];
+  wq[wq_offset(m, C) + q] = a == b ? p : 2.0 * p;
+}
+
+// Diagonal atom block element (A, pq): Coulomb over every atom plus one-center exchange.
+// Returns the element's share of E_el.
+__device__ inline double fock_diag_task(const MolView& m, const double* wq, double* Fs,
+                                        int64_t ld, int t) {
+  const int A = t / 10, pq = t % 10;
+  const int sA = m.slot[A];
+  if (sA == 0 && pq) return 0.0;
+  const int a = pair_first(pq), b = pair_second(pq), fA = m.first[A];
+  double J = 0.0;
+  for (int C = 0; C < m.natoms; ++C) {
+    const int sC = m.slot[C];
+    const double* w = wq + wq_offset(m, C);
+    if (sA == 0) {
+      if (sC == 0) {
+        J += *blk_ptr(m, A > C ? A : C, A > C ? C : A) * w[0];
+      } else {
+        const double* I = blk_ptr(m, A > C ? A : C, A > C ? C : A);
+#pragma unroll
+        for (int q = 0; q < 10; ++q) J += I[q] * w[q];
+      }
+    } else if (sC == 0) {
+      J += blk_ptr(m, A > C ? A : C, A > C ? C : A)[pq] * w[0];
+    } else if (A >= C) {
+      const double* I = blk_ptr(m, A, C) + 10 * pq;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) J += I[q] * w[q];
+    } else {
+      const double* I = blk_ptr(m, C, A) + pq;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) J += I[10 * q] * w[q];
+    }
+  }
+  // one-center exchange -1/2 sum_{lam,sig in A} P_lam_sig (mu lam|nu sig)
+  double K = 0.0;
+  const int nA = nao_of_slot(sA);
+  for (int l = 0; l < nA; ++l)
+    for (int s = 0; s < nA; ++s) {
+      const double x = one_center_value(sA, a < l ? a : l, a < l ? l : a, b < s ? b : s, b < s ? s : b);
+      if (x != 0.0) K += m.P[pk(fA + l, fA + s)] * x;
+    }
+  const int i = fA + b, j = fA + a;  // i >= j
+  const int64_t ij = tri(i) + j;
+  const double h = m.H[ij], fv = h + (J - 0.5 * K);
+  m.F[ij] = fv;
+  if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
+  return m.P[ij] * (h + fv) * (i == j ? 0.5 : 1.0);
+}
+
+// Off-diagonal atom block (A > B): two-center exchange only.  Returns its share of E_el.
+__device__ inline double fock_pair_task(const MolView& m, double* Fs, int64_t ld, int A, int B) {
+  const int sA = m.slot[A], sB = m.slot[B], fA = m.first[A], fB = m.first[B];
+  const double* I = blk_ptr(m, A, B);
+  const int nA = nao_of_slot(sA), nB = nao_of_slot(sB);
+  double Pab[16];
+  for (int l = 0; l < nA; ++l)
+    for (int s = 0; s < nB; ++s) Pab[4 * l + s] = m.P[tri(fA + l) + fB + s];
+  double e = 0.0;
+  for (int mu = 0; mu < nA; ++mu)
+    for (int nu = 0; nu < nB; ++nu) {
+      double g = 0.0;
+      if (sA != 0 && sB != 0) {
+        for (int l = 0; l < 4; ++l) {
+          const double* Ir = I + 10 * pair_index(mu, l);
+#pragma unroll
+          for (int s = 0; s < 4; ++s) g += Pab[4 * l + s] * Ir[pair_index(nu, s)];
+        }
+      } else if (sA != 0) {  // B is H: (mu lam | s_B s_B), block column = pair(mu, lam)
+        for (int l = 0; l < 4; ++l) g += Pab[4 * l] * I[pair_index(mu, l)];
+      } else if (sB != 0) {  // A is H: (s_A s_A | nu sig)
+        for (int s = 0; s < 4; ++s) g += Pab[s] * I[pair_index(nu, s)];
+      } else {
+        g = Pab[0] * I[0];
+      }
+      const int i = fA + mu, j = fB + nu;
+      const int64_t ij = tri(i) + j;
+      const double h = m.H[ij], fv = h - 0.5 * g;
+      m.F[ij] = fv;
+      if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
+      e += m.P[ij] * (h + fv);
+    }
+  return e;
+}
 
 template <int NT>
 __device__ double block_fock_energy(const MolView& m, double* Fs, int ld, double* wq,
                                     double* red) {
-  // pair densities
-  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) {
-    const int C = t / 10, q = t % 10;
-    const int s = m.slot[C];
-    if (s == 0 && q) continue;
-    const int a = pair_first(q), b = pair_second(q), f = m.first[C];
-    const double p = m.P[tri(f + b) + f + a];
-    wq[wq_offset(m, C) + q] = a == b ? p : 2.0 * p;
-  }
+  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) pair_density_task(m, wq, t);
   __syncthreads();
   double e = 0.0;
-  // diagonal atom blocks: task (A, pq)
-  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) {
-    const int A = t / 10, pq = t % 10;
-    const int sA = m.slot[A];
-    if (sA == 0 && pq) continue;
-    const int a = pair_first(pq), b = pair_second(pq), fA = m.first[A];
-    double J = 0.0;
-    for (int C = 0; C < m.natoms; ++C) {
-      const int sC = m.slot[C];
-      const double* w = wq + wq_offset(m, C);
-      if (sA == 0) {
-        if (sC == 0) {
-          J += *blk_ptr(m, A > C ? A : C, A > C ? C : A) * w[0];
-        } else {
-          const double* I = blk_ptr(m, A > C ? A : C, A > C ? C : A);
-#pragma unroll
-          for (int q = 0; q < 10; ++q) J += I[q] * w[q];
-        }
-      } else if (sC == 0) {
-        J += blk_ptr(m, A > C ? A : C, A > C ? C : A)[pq] * w[0];
-      } else if (A >= C) {
-        const double* I = blk_ptr(m, A, C) + 10 * pq;
-#pragma unroll
-        for (int q = 0; q < 10; ++q) J += I[q] * w[q];
-      } else {
-        const double* I = blk_ptr(m, C, A) + pq;
-#pragma unroll
-        for (int q = 0; q < 10; ++q) J += I[10 * q] * w[q];
-      }
-    }
-    // one-center exchange -1/2 sum_{lam,sig in A} P_lam_sig (mu lam|nu sig)
-    double K = 0.0;
-    const int nA = nao_of_slot(sA);
-    for (int l = 0; l < nA; ++l)
-      for (int s = 0; s < nA; ++s) {
-        const double x = one_center_value(sA, a < l ? a : l, a < l ? l : a, b < s ? b : s, b < s ? s : b);
-        if (x != 0.0) K += m.P[pk(fA + l, fA + s)] * x;
-      }
-    const int i = fA + b, j = fA + a;  // i >= j
-    const int64_t ij = tri(i) + j;
-    const double h = m.H[ij], fv = h + (J - 0.5 * K);
-    m.F[ij] = fv;
-    if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
-    e += m.P[ij] * (h + fv) * (i == j ? 0.5 : 1.0);
-  }
-  // off-diagonal atom blocks: two-center exchange only
+  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) e += fock_diag_task(m, wq, Fs, ld, t);
   const int64_t np = tri(m.natoms);
   for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
     int A, B;
     tri_inverse(p, A, B);
-    if (A == B) continue;
-    const int sA = m.slot[A], sB = m.slot[B], fA = m.first[A], fB = m.first[B];
-    const double* I = blk_ptr(m, A, B);
-    const int nA = nao_of_slot(sA), nB = nao_of_slot(sB);
-    double Pab[16];
-    for (int l = 0; l < nA; ++l)
-      for (int s = 0; s < nB; ++s) Pab[4 * l + s] = m.P[tri(fA + l) + fB + s];
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nB; ++nu) {
-        double g = 0.0;
-        if (sA != 0 && sB != 0) {
-          for (int l = 0; l < 4; ++l) {
-            const double* Ir = I + 10 * pair_index(mu, l);
-#pragma unroll
-            for (int s = 0; s < 4; ++s) g += Pab[4 * l + s] * Ir[pair_index(nu, s)];
-          }
-        } else if (sA != 0) {  // B is H: (mu lam | s_B s_B), block column = pair(mu, lam)
-          for (int l = 0; l < 4; ++l) g += Pab[4 * l] * I[pair_index(mu, l)];
-        } else if (sB != 0) {  // A is H: (s_A s_A | nu sig)
-          for (int s = 0; s < 4; ++s) g += Pab[s] * I[pair_index(nu, s)];
-        } else {
-          g = Pab[0] * I[0];
-        }
-        const int i = fA + mu, j = fB + nu;
-        const int64_t ij = tri(i) + j;
-        const double h = m.H[ij], fv = h - 0.5 * g;
-        m.F[ij] = fv;
-        if (Fs) { Fs[i * ld + j] = fv; Fs[j * ld + i] = fv; }
-        e += m.P[ij] * (h + fv);
-      }
+    if (A != B) e += fock_pair_task(m, Fs, ld, A, B);
   }
   return block_sum<NT>(e, red);
 }
@@ -286,30 +299,34 @@ __device__ inline void block_guess(const MolView& m) {
   }
 }
 
-// Core-core repulsion, sum over A < B (corecorerepulsion.cpp:12-65).
+// Core-core repulsion of atoms Al < Bh (corecorerepulsion.cpp:12-65):
+// Z_A Z_B (s_A s_A|s_B s_B) f(R), R in Angstrom; N-H / O-H use 1 + R exp(-alpha_X R) + exp(-alpha_H R).
+__device__ inline double core_core_pair(const MolView& m, int Bh, int Al) {
+  const int sa = m.slot[Al], sb = m.slot[Bh];
+  const double gam = *blk_ptr(m, Bh, Al);
+  const double* pa = m.pos + 3 * Al;
+  const double* pb = m.pos + 3 * Bh;
+  const double dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
+  const double r = sqrt(dx * dx + dy * dy + dz * dz) * kBohr2Ang;
+  const int za = c_elem[sa].z, zb = c_elem[sb].z;
+  double f;
+  if (zb == 1 && (za == 7 || za == 8))
+    f = 1.0 + r * exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
+  else if (za == 1 && (zb == 7 || zb == 8))
+    f = 1.0 + r * exp(-c_elem[sb].alpha * r) + exp(-c_elem[sa].alpha * r);
+  else
+    f = 1.0 + exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
+  return (double)(c_elem[sa].core * c_elem[sb].core) * gam * f;
+}
+
 template <int NT>
 __device__ double block_core_core(const MolView& m, double* red) {
   double e = 0.0;
   const int64_t np = tri(m.natoms);
   for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
-    int Bh, Al;  // Bh > Al
+    int Bh, Al;
     tri_inverse(p, Bh, Al);
-    if (Bh == Al) continue;
-    const int sa = m.slot[Al], sb = m.slot[Bh];
-    const double gam = *blk_ptr(m, Bh, Al);
-    const double* pa = m.pos + 3 * Al;
-    const double* pb = m.pos + 3 * Bh;
-    const double dx = pa[0] - pb[0], dy = pa[1] - pb[1], dz = pa[2] - pb[2];
-    const double r = sqrt(dx * dx + dy * dy + dz * dz) * kBohr2Ang;
-    const int za = c_elem[sa].z, zb = c_elem[sb].z;
-    double f;
-    if (zb == 1 && (za == 7 || za == 8))
-      f = 1.0 + r * exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
-    else if (za == 1 && (zb == 7 || zb == 8))
-      f = 1.0 + r * exp(-c_elem[sb].alpha * r) + exp(-c_elem[sa].alpha * r);
-    else
-      f = 1.0 + exp(-c_elem[sa].alpha * r) + exp(-c_elem[sb].alpha * r);
-    e += (double)(c_elem[sa].core * c_elem[sb].core) * gam * f;
+    if (Bh != Al) e += core_core_pair(m, Bh, Al);
   }
   return block_sum<NT>(e, red);
 }

@@ -1,0 +1,80 @@
+"""The grid-wide path (whole GPU on one molecule, host-driven SCF, cooperative Jacobi):
+forced onto the small golden cases, and on its own above nao 160 (C60, C100H202)."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+import semigpu_b200 as sg
+from semigpu_b200 import geometry as geo
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+with open(os.path.join(GOLDEN, "reference_cases.json")) as _fh:
+    CASES = json.load(_fh)["cases"]
+_M = np.load(os.path.join(GOLDEN, "reference_matrices.npz"))
+MATRIX_CASES = sorted({k.rsplit("/", 1)[0] for k in _M.files})
+
+
+def _mol(ctx, key, path=sg.PATH_AUTO):
+    c = CASES[key]
+    m = sg.Molecule(ctx, np.array(c["Z"], np.int32), np.array(c["xyz"]))
+    m.set_path(path)
+    return m, c
+
+
+@pytest.mark.parametrize("key", MATRIX_CASES[::3])
+def test_grid_path_matrices(gpu_ctx, key):
+    m, c = _mol(gpu_ctx, key, sg.PATH_GRID)
+    m.two_center()
+    np.testing.assert_allclose(m.get(sg.BLOCKS), _M[f"{key}/blocks"], rtol=0, atol=1e-8)
+    m.hcore()
+    np.testing.assert_allclose(m.get(sg.HCORE), _M[f"{key}/H"], rtol=0, atol=1e-8)
+    F, e = m.fock(_M[f"{key}/P0"])
+    np.testing.assert_allclose(F, _M[f"{key}/F0"], rtol=0, atol=1e-8)
+    r = m.scf(tol=c["tol"], max_iter=100)
+    assert r["n_iter"] == c["n_iter"]
+    np.testing.assert_allclose(r["energies"], c["energies"], rtol=0, atol=1e-6)
+    np.testing.assert_allclose(m.get(sg.DENSITY), _M[f"{key}/P"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(m.get(sg.EIGVAL), _M[f"{key}/eig"], rtol=0, atol=1e-8)
+    assert abs(m.core_core() - c["E_cc"]) < 1e-6
+
+
+def test_c60_auto_grid(gpu_ctx):
+    """nao 240: above the CTA path, so AUTO runs the grid path; reference at its 5e-3 default."""
+    key = "fixture/C60-Ih@0.005"
+    m, c = _mol(gpu_ctx, key)
+    r = m.run(tol=c["tol"])
+    assert r["n_iter"] == c["n_iter"]
+    assert abs(r["E_el"] - c["E_el"]) < 1e-6
+    assert abs(r["E_cc"] - c["E_cc"]) < 1e-6
+
+
+def test_grid_equals_cta(gpu_ctx):
+    mol = geo.polyene(30, np.random.default_rng(2))  # nao 152: both paths apply
+    a = sg.Molecule.from_geometry(gpu_ctx, mol)
+    a.set_path(sg.PATH_CTA)
+    b = sg.Molecule.from_geometry(gpu_ctx, mol)
+    b.set_path(sg.PATH_GRID)
+    ra, rb = a.run(tol=1e-6), b.run(tol=1e-6)
+    assert ra["n_iter"] == rb["n_iter"]
+    assert abs(ra["E_tot"] - rb["E_tot"]) < 1e-8
+    np.testing.assert_allclose(a.get(sg.DENSITY), b.get(sg.DENSITY), rtol=0, atol=1e-9)
+
+
+def test_c100h202_against_oracle(gpu_ctx, oracle_mod):
+    """Config C100H202 (302 atoms, 602 AOs, 301 occupied), tol 1e-6 eV."""
+    mol = geo.alkane_c2(0)
+    assert (mol.natoms, mol.nao, mol.nocc) == (302, 602, 301)
+    m = sg.Molecule.from_geometry(gpu_ctx, mol)
+    r = m.run(tol=1e-6)
+    o = oracle_mod.scf(mol.Z, mol.xyz, tol=1e-6)
+    assert r["status"] == 0 and r["converged"]
+    assert r["n_iter"] == o["n_iter"]
+    assert abs(r["E_el"] - o["E_el"]) < 1e-6
+    assert abs(r["E_cc"] - o["E_cc"]) < 1e-6
+    np.testing.assert_allclose(m.get(sg.FOCK), o["F"], rtol=0, atol=1e-8)
