@@ -64,6 +64,31 @@ const char *sgb_status_string(int status);
 /* Bytes of device memory currently held by the context's molecules and batches. */
 size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
 
+/* ---- MNDO element data ------------------------------------------------------------------ */
+/* Parameters of element Z (1, 6, 7, 8) as used by the engine, in the units of
+ * MNDO_parameters.cpp:47-122 (eV, bohr, 1/Angstrom, kcal/mol).  Replaces reading the public
+ * arrays of MNDOparameter. */
+#define SGB_P_USS 0
+#define SGB_P_UPP 1
+#define SGB_P_ZS 2
+#define SGB_P_BETAS 3
+#define SGB_P_BETAP 4
+#define SGB_P_ALPHA 5
+#define SGB_P_GSS 6
+#define SGB_P_GPP 7
+#define SGB_P_GSP 8
+#define SGB_P_GP2 9
+#define SGB_P_HSP 10
+#define SGB_P_DD1 11
+#define SGB_P_DD2 12
+#define SGB_P_RHO0 13
+#define SGB_P_RHO1 14
+#define SGB_P_RHO2 15
+#define SGB_P_HEAT 16
+#define SGB_P_EISOL 17
+#define SGB_PARAM_COUNT 18
+int sgb_mndo_parameters(int Z, double *values);
+
 /* ---- one molecule: the reference's stage API ------------------------------------------- */
 /* Replaces ReadXYZFile output handling + ListAtomicOrbitals::SetOrbitals
  * (atomicOrbitals.cpp:76-119) + TwoCenterIntegral::Alloc4AllTwoCenterIntegral

@@ -38,6 +38,7 @@ SIGNATURES = {
     "sgb_last_error": (ctypes.c_char_p, [_VP]),
     "sgb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
+    "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
     "sgb_mol_destroy": (ctypes.c_int, [_VP]),
     "sgb_mol_info": (ctypes.c_int, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),

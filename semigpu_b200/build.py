@@ -1,6 +1,7 @@
-"""Builds libsemigpu_b200.so in-tree with nvcc for sm_100a (B200).
+"""Builds, in-tree, the CUDA library libsemigpu_b200.so (nvcc, sm_100a) and on top of it the
+C++ host API libsemigpu_host.so plus the `semiGPU` command-line program.
 
-    python -m semigpu_b200.build [--verbose]
+    python -m semigpu_b200.build [--verbose] [--force]
 """
 from __future__ import annotations
 
@@ -16,6 +17,13 @@ FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-li
          "-Xcompiler", "-fPIC,-O2", "-shared", "--expt-relaxed-constexpr"]
 
 
+HOST_DIR = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libsemigpu_host.so")
+CLI = os.path.join(HERE, "semiGPU")
+INC = os.path.join(os.path.dirname(HERE), "include")
+CXX = os.environ.get("CXX", "g++")
+
+
 def sources():
     d = os.path.join(HERE, "csrc")
     return [os.path.join(d, f) for f in sorted(os.listdir(d)) if f.endswith((".cu", ".cuh", ".h"))] + [
@@ -29,6 +37,25 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(s) <= t for s in sources())
 
 
+def build_host(verbose: bool = False) -> None:
+    """The C++ façade (reference class names) and the CLI, linked to the CUDA library."""
+    common = ["-O2", "-std=c++17", "-fPIC", f"-I{INC}", f"-I{HOST_DIR}"]
+    lib = [f"-L{HERE}", "-lsemigpu_b200", "-Wl,-rpath,$ORIGIN"]
+    cmds = [[CXX, *common, "-shared", os.path.join(HOST_DIR, "semigpu.cpp"), *lib, "-o", HOST_LIB],
+            [CXX, *common, os.path.join(HOST_DIR, "semiGPU.cc"), f"-L{HERE}", "-lsemigpu_host",
+             *lib, "-o", CLI]]
+    for cmd in cmds:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+
+
+def host_up_to_date() -> bool:
+    srcs = [os.path.join(HOST_DIR, f) for f in os.listdir(HOST_DIR)] + [OUT]
+    return all(os.path.exists(p) for p in (HOST_LIB, CLI)) and all(
+        os.path.getmtime(s) <= min(os.path.getmtime(HOST_LIB), os.path.getmtime(CLI)) for s in srcs)
+
+
 def build(verbose: bool = False, force: bool = False) -> str:
     if force or not up_to_date():
         cmd = [NVCC, *FLAGS, SRC, "-o", OUT]
@@ -36,6 +63,8 @@ def build(verbose: bool = False, force: bool = False) -> str:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    if force or not host_up_to_date():
+        build_host(verbose)
     return OUT
 
 

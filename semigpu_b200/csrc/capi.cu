@@ -617,6 +617,22 @@ const char* sgb_status_string(int s) {
 
 const char* sgb_last_error(const sgb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int sgb_mndo_parameters(int Z, double* v) {
+  const int s = slot_of(Z);
+  if (s < 0 || !v) return SGB_E_ELEMENT;
+  // exponent, heat of formation of the atom and its computed total energy: parameters the
+  // reference stores but its SCF path does not use (MNDO_parameters.cpp:47-122)
+  static const double zs[4] = {1.3319670, 1.7875370, 2.25561400, 2.69990500};
+  static const double heat[4] = {52.102, 170.89, 113.00000000, 59.55900000};
+  static const double eisol[4] = {-11.9062760, -120.500606, -202.56620100, -317.86850600};
+  const ElemParams& e = kElemHost[s];
+  const double vals[SGB_PARAM_COUNT] = {e.uss, e.upp, zs[s], e.beta_s, e.beta_p, e.alpha, e.gss,
+                                        e.gpp, e.gsp, e.gp2, e.hsp, e.dd1, e.dd2, e.rho[0],
+                                        e.rho[1], e.rho[2], heat[s], eisol[s]};
+  for (int k = 0; k < SGB_PARAM_COUNT; ++k) v[k] = vals[k];
+  return SGB_OK;
+}
+
 size_t sgb_ctx_bytes_in_use(const sgb_ctx* ctx) { return ctx ? ctx->in_use : 0; }
 
 int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {

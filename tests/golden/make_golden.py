@@ -100,12 +100,33 @@ def readers():
     return res
 
 
+CLI_FIXTURES = ("04_pyridine", "03_formaldehyde", "02_benzene", "01_h2")
+
+
+def cli_outputs():
+    """The unmodified reference CLI's printout (oracle/_ref/semiGPU) on a few fixtures."""
+    import subprocess
+
+    out = {}
+    for base in CLI_FIXTURES:
+        path = os.path.join(FIXTURE_DIR, base + ".xyz")
+        r = subprocess.run([oracle.REF_CLI, path], capture_output=True, text=True, check=True,
+                           env=dict(os.environ, OPENBLAS_NUM_THREADS="1"))
+        out[base] = {"xyz": open(path).read(), "stdout": r.stdout}
+    with open(os.path.join(HERE, "reference_cli.json"), "w") as fh:
+        json.dump(out, fh, indent=0)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--c2", action="store_true")
+    ap.add_argument("--cli-only", action="store_true")
     ap.add_argument("--jobs", type=int, default=os.cpu_count())
     args = ap.parse_args()
     oracle.build()
+    cli_outputs()
+    if args.cli_only:
+        return
     todo = cases(args.c2)
     todo.sort(key=lambda c: -len(c[1]))
     summaries, mats = {}, {}
