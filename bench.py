@@ -331,7 +331,8 @@ def run_ours(args):
         achieved = flops / (my_ms / args.steps / 1e3) / 1e12
         traffic = load_traffic()
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": None, "kernel": "k_batch_scf<512>",
+                "frac": achieved / peak, "traffic": None,
+                "kernel": "k_batch_scf (one persistent launch per nao size class; FP64 pipe)",
                 "peak_source": peak_src,
                 "numerator": "sum over molecules of n_iter*((10/3)N^3 + 2 N^2 nocc) FP64 flops"}
         if traffic:
@@ -382,7 +383,7 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * nat_total,
                     "d2h_bytes_per_step": nb * (8 + 8 + 4 + 4 + 4)},
             "clocks": clk,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * batch.launches(),
         }
         print(json.dumps(line))
     batch.close()

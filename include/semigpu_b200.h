@@ -146,6 +146,8 @@ int sgb_batch_results(sgb_ctx *ctx, sgb_batch *b, double *e_el, double *e_cc, in
 int sgb_run_molecules(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, const double *xyz,
                       double tol, int max_iter, double *e_el, double *e_cc, int *n_iter,
                       int *converged, int *status);
+/* Kernel launches one sgb_batch_run makes (one persistent launch per occupied size class). */
+int sgb_batch_launches(const sgb_batch *b, int *launches);
 /* Device-time of the last sgb_batch_run in milliseconds (CUDA events on the context stream). */
 int sgb_batch_last_ms(const sgb_batch *b, float *ms);
 /* Per-molecule device timestamps (ns, %globaltimer) of the last run: when its CTA started the

@@ -57,6 +57,7 @@ SIGNATURES = {
     "sgb_run_molecules": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.c_double,
                                          ctypes.c_int, _D, _D, _I, _I, _I]),
     "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "sgb_batch_launches": (ctypes.c_int, [_VP, _I]),
     "sgb_batch_device_coordinates": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "sgb_batch_timestamps": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_ulonglong),
                                             ctypes.POINTER(ctypes.c_ulonglong)]),
@@ -254,6 +255,12 @@ class Batch:
                                                _i(cv), _i(st)), "sgb_batch_results")
         return {"E_el": eel, "E_cc": ecc, "E_tot": eel + ecc, "n_iter": it,
                 "converged": cv.astype(bool), "status": st}
+
+    def launches(self) -> int:
+        """Kernel launches per run (one persistent launch per occupied size class)."""
+        n = ctypes.c_int()
+        lib().sgb_batch_launches(self.h, ctypes.byref(n))
+        return n.value
 
     def last_ms(self) -> float:
         ms = ctypes.c_float()

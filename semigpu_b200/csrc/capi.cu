@@ -918,6 +918,14 @@ int sgb_batch_timestamps(sgb_ctx* ctx, sgb_batch* b, unsigned long long* t_begin
   return sgb_ctx_synchronize(ctx);
 }
 
+int sgb_batch_launches(const sgb_batch* b, int* launches) {
+  if (!b || !launches) return SGB_E_ARG;
+  int n = 0;
+  for (int c = 0; c < kNumClasses; ++c) n += b->class_count[c] > 0;
+  *launches = n;
+  return SGB_OK;
+}
+
 int sgb_batch_set_profiling(sgb_batch* b, int on) {
   if (!b) return SGB_E_ARG;
   b->profiling = on != 0;
