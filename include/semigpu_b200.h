@@ -166,6 +166,25 @@ int sgb_batch_stage_cycles(sgb_ctx *ctx, sgb_batch *b, unsigned long long *cycle
  * stage inputs themselves. */
 int sgb_batch_device_coordinates(sgb_batch *b, void **dptr);
 
+/* ---- one molecule without any device allocation ----------------------------------------- */
+/* No counterpart in the reference.  For callers that may not allocate device memory: code
+ * running inside a host framework that owns the GPU's memory through its own pool and forbids
+ * other allocations, or code that must not allocate after it has started.  Runs one molecule's
+ * whole calculation (integrals, Hcore, SCF to |dE| < tol within max_iter steps, core-core
+ * repulsion) on the CURRENT device, on `stream` (a cudaStream_t; NULL = the default stream), and
+ * returns when the results are in the host outputs (any output pointer may be NULL).  It calls
+ * no cudaMalloc / cudaFree and no allocating library routine: all device scratch is a 1 MiB
+ * static array that every GPU which loads this library holds until the process exits.
+ * Limit: at most 128 atoms and 128 atomic orbitals (e.g. C32, C20H42); larger molecules are
+ * rejected with SGB_E_UNSUPPORTED before any GPU work.  The first call on a device does that
+ * device's set-up (loads the MNDO tables, looks up the scratch's device address), so it should
+ * come before any stream capture.  Every call on a device uses the same scratch, which keeps the
+ * previous call's contents: calls whose GPU work overlaps (other streams, other host threads)
+ * race and must be serialised by the caller.  Returns SGB_OK, SGB_E_EIG, SGB_E_NAN, or an error. */
+int sgb_scf_noalloc(int natoms, const int *Z, const double *xyz, double tol, int max_iter,
+                    void *stream, double *e_el, double *e_cc, int *n_iter, int *converged,
+                    int *status);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,8 @@ SIGNATURES = {
                                          ctypes.c_int, _D, _D, _I, _I, _I]),
     "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
     "sgb_batch_launches": (ctypes.c_int, [_VP, _I]),
+    "sgb_scf_noalloc": (ctypes.c_int, [ctypes.c_int, _I, _D, ctypes.c_double, ctypes.c_int, _VP,
+                                       _D, _D, _I, _I, _I]),
     "sgb_batch_device_coordinates": (ctypes.c_int, [_VP, ctypes.POINTER(_VP)]),
     "sgb_batch_timestamps": (ctypes.c_int, [_VP, _VP, ctypes.POINTER(ctypes.c_ulonglong),
                                             ctypes.POINTER(ctypes.c_ulonglong)]),

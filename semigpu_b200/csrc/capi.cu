@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -313,7 +314,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
 
 // One kernel instantiation per (threads per CTA, eigenvector column registers per lane).
 template <int NT, int CR>
-cudaError_t launch_kernel(sgb_ctx* ctx, const BatchArgs& a, size_t smem, cudaStream_t st) {
+cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStream_t st) {
   auto* k = k_batch_scf<NT, CR>;
   cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -321,26 +322,26 @@ cudaError_t launch_kernel(sgb_ctx* ctx, const BatchArgs& a, size_t smem, cudaStr
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
-  const int grid = std::min(a.nmol, per_sm * ctx->num_sms);
+  const int grid = std::min(a.nmol, per_sm * num_sms);
   k<<<grid, NT, smem, st>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_class(sgb_ctx* ctx, const BatchArgs& a, int cr, int threads, size_t smem,
+cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
                          cudaStream_t st) {
   if (threads == 512) {
     switch (cr) {
-      case 2: return launch_kernel<512, 2>(ctx, a, smem, st);
-      case 3: return launch_kernel<512, 3>(ctx, a, smem, st);
-      case 4: return launch_kernel<512, 4>(ctx, a, smem, st);
-      default: return launch_kernel<512, 5>(ctx, a, smem, st);
+      case 2: return launch_kernel<512, 2>(num_sms, a, smem, st);
+      case 3: return launch_kernel<512, 3>(num_sms, a, smem, st);
+      case 4: return launch_kernel<512, 4>(num_sms, a, smem, st);
+      default: return launch_kernel<512, 5>(num_sms, a, smem, st);
     }
   }
   switch (cr) {
-    case 2: return launch_kernel<256, 2>(ctx, a, smem, st);
-    case 3: return launch_kernel<256, 3>(ctx, a, smem, st);
-    case 4: return launch_kernel<256, 4>(ctx, a, smem, st);
-    default: return launch_kernel<256, 5>(ctx, a, smem, st);
+    case 2: return launch_kernel<256, 2>(num_sms, a, smem, st);
+    case 3: return launch_kernel<256, 3>(num_sms, a, smem, st);
+    case 4: return launch_kernel<256, 4>(num_sms, a, smem, st);
+    default: return launch_kernel<256, 5>(num_sms, a, smem, st);
   }
 }
 
@@ -392,7 +393,7 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
     const size_t smem = (ac.mat_doubles + extra_doubles(ac.nmax)) * sizeof(double);
     cudaStream_t cs = ctx->aux[c];
     CUDA_TRY(ctx, cudaStreamWaitEvent(cs, b->ev0, 0));
-    cudaError_t e = launch_class(ctx, ac, kClasses[c].cr, ctx->class_threads[c], smem, cs);
+    cudaError_t e = launch_class(ctx->num_sms, ac, kClasses[c].cr, ctx->class_threads[c], smem, cs);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "k_batch_scf launch");
     CUDA_TRY(ctx, cudaEventRecord(ctx->joined[c], cs));
     CUDA_TRY(ctx, cudaStreamWaitEvent(st, ctx->joined[c], 0));
@@ -594,6 +595,44 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
   }
   return status;
 }
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free single-molecule run (sgb_scf_noalloc).  All of its device scratch -- the
+// molecule descriptor, atom arrays, integral blocks, Hcore / P / F, the two n x n matrices and
+// the results -- is carved out of one file-scope array that exists for as long as the library
+// is loaded.  Host code never touches g_noalloc_scratch by name: its device address comes from
+// cudaGetSymbolAddress, fetched once per device.
+constexpr int kNoAllocMaxNao = 128;
+constexpr int kNoAllocMaxAtoms = 128;
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB per GPU
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+struct NoAllocDevice {
+  bool ready = false;
+  unsigned char* scratch = nullptr;
+  int num_sms = 0;
+};
+NoAllocDevice g_noalloc[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
+
+// Everything the host writes before a run, staged in one contiguous block (one copy).
+struct NoAllocHeader {
+  MolDesc desc;
+  int order;
+  int counter[kNumClasses];
+  int8_t slot[kNoAllocMaxAtoms];
+  int first[kNoAllocMaxAtoms];
+  int hb[kNoAllocMaxAtoms];
+  int64_t row_off[kNoAllocMaxAtoms];
+  double xyz[3 * kNoAllocMaxAtoms];
+};
+
+struct NoAllocResults {
+  double e_el, e_cc;
+  int n_iter, converged, status, pad;
+};
 
 }  // namespace
 
@@ -966,6 +1005,133 @@ int sgb_run_molecules(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, c
   rc = sgb_batch_run(ctx, b, tol, max_iter);
   if (rc) return rc;
   return sgb_batch_results(ctx, b, e_el, e_cc, n_iter, converged, status);
+}
+
+int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int max_iter,
+                    void* stream, double* e_el, double* e_cc, int* n_iter, int* converged,
+                    int* status) {
+  if (natoms <= 0 || !Z || !xyz || max_iter < 0 || !(tol >= 0.0)) return SGB_E_ARG;
+  if (natoms > kNoAllocMaxAtoms) {
+    fprintf(stderr, "sgb_scf_noalloc: %d atoms, the allocation-free path takes at most %d\n",
+            natoms, kNoAllocMaxAtoms);
+    return SGB_E_UNSUPPORTED;
+  }
+  // host-side layout on the stack (no heap, no device allocation)
+  NoAllocHeader h;
+  memset(&h, 0, sizeof h);
+  int nao = 0, nel = 0, nheavy = 0;
+  int64_t roff = 0;
+  for (int a = 0; a < natoms; ++a) {
+    const int s = slot_of(Z[a]);
+    if (s < 0) return SGB_E_ELEMENT;
+    const bool heavy = s != 0;
+    h.slot[a] = (int8_t)s;
+    h.first[a] = nao;
+    h.hb[a] = nheavy;
+    h.row_off[a] = roff;
+    const int nh = nheavy + (heavy ? 1 : 0), nl = a + 1 - nh;
+    roff += (int64_t)nh * (heavy ? 100 : 10) + (int64_t)nl * (heavy ? 10 : 1);
+    nao += heavy ? 4 : 1;
+    nel += s == 0 ? 1 : (Z[a] - 2);
+    nheavy += heavy ? 1 : 0;
+  }
+  if (nao > kNoAllocMaxNao) {
+    fprintf(stderr, "sgb_scf_noalloc: %d atomic orbitals, the allocation-free path takes at most %d\n",
+            nao, kNoAllocMaxNao);
+    return SGB_E_UNSUPPORTED;
+  }
+  memcpy(h.xyz, xyz, sizeof(double) * 3 * natoms);
+  // device layout inside the static scratch
+  size_t off = 0;
+  auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
+  const size_t o_head = take(sizeof(NoAllocHeader)), o_pos = take(24 * (size_t)natoms),
+               o_res = take(sizeof(NoAllocResults)), o_ints = take(8 * (size_t)roff),
+               o_H = take(8 * (size_t)tri(nao)), o_P = take(8 * (size_t)tri(nao)),
+               o_F = take(8 * (size_t)tri(nao)), o_V = take(8 * (size_t)nao * nao),
+               o_T = take(8 * (size_t)nao * nao), o_eig = take(8 * (size_t)nao);
+  if (off > kNoAllocScratchBytes) {
+    fprintf(stderr, "sgb_scf_noalloc: molecule needs %zu bytes of scratch, %zu available\n", off,
+            kNoAllocScratchBytes);
+    return SGB_E_UNSUPPORTED;
+  }
+  // per-device set-up on the first call: constant tables and the scratch's device address
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) return SGB_E_CUDA;
+  NoAllocDevice& nd = g_noalloc[dev];
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!nd.ready) {
+      void* ptr = nullptr;
+      if (upload_tables() != cudaSuccess) return SGB_E_CUDA;
+      if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return SGB_E_CUDA;
+      if (cudaDeviceGetAttribute(&nd.num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return SGB_E_CUDA;
+      nd.scratch = static_cast<unsigned char*>(ptr);
+      nd.ready = true;
+    }
+  }
+  unsigned char* base = nd.scratch;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  h.desc.natoms = natoms;
+  h.desc.nao = nao;
+  h.desc.nocc = nel / 2;
+  h.desc.nheavy = nheavy;
+  h.desc.nblk = roff;  // all offsets of the views below are relative to their own buffers
+  h.order = 0;         // counter[] stays zero: it must start at zero every run
+  if (cudaMemcpyAsync(base + o_head, &h, sizeof h, cudaMemcpyHostToDevice, st) != cudaSuccess)
+    return SGB_E_CUDA;
+  NoAllocHeader* dh = reinterpret_cast<NoAllocHeader*>(base + o_head);
+  double* pos = reinterpret_cast<double*>(base + o_pos);
+  k_ang_to_bohr<<<1, 128, 0, st>>>(dh->xyz, pos, 3 * natoms);
+  NoAllocResults* dr = reinterpret_cast<NoAllocResults*>(base + o_res);
+  BatchArgs a;
+  a.nmol = 1;
+  a.mols = &dh->desc;
+  a.order = &dh->order;
+  a.counter = dh->counter;
+  a.slot = dh->slot;
+  a.pos = pos;
+  a.first = dh->first;
+  a.row_off = dh->row_off;
+  a.hb = dh->hb;
+  a.ints = reinterpret_cast<double*>(base + o_ints);
+  a.H = reinterpret_cast<double*>(base + o_H);
+  a.P = reinterpret_cast<double*>(base + o_P);
+  a.F = reinterpret_cast<double*>(base + o_F);
+  a.V = reinterpret_cast<double*>(base + o_V);
+  a.T = reinterpret_cast<double*>(base + o_T);
+  a.eig = reinterpret_cast<double*>(base + o_eig);
+  a.e_el = &dr->e_el;
+  a.e_cc = &dr->e_cc;
+  a.n_iter = &dr->n_iter;
+  a.converged = &dr->converged;
+  a.status = &dr->status;
+  a.hist = nullptr;
+  a.hist_stride = 0;
+  a.tol = tol;
+  a.max_iter = max_iter;
+  a.nmax = nao;
+  a.mat_doubles = mat_doubles_for(nao);
+  a.sorted_vectors = 0;
+  a.stages = STAGE_ALL;
+  a.t_begin = nullptr;
+  a.t_end = nullptr;
+  a.stage_cycles = nullptr;
+  const int c = class_of(nao);
+  const size_t smem = (a.mat_doubles + extra_doubles(a.nmax)) * sizeof(double);
+  if (launch_class(nd.num_sms, a, kClasses[c].cr, kClasses[c].threads, smem, st) != cudaSuccess)
+    return SGB_E_CUDA;
+  NoAllocResults r;
+  if (cudaMemcpyAsync(&r, dr, sizeof r, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return SGB_E_CUDA;
+  if (e_el) *e_el = r.e_el;
+  if (e_cc) *e_cc = r.e_cc;
+  if (n_iter) *n_iter = r.n_iter;
+  if (converged) *converged = r.converged;
+  const int st_code = r.status == MOL_OK ? SGB_OK : r.status == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN;
+  if (status) *status = st_code;
+  return st_code;
 }
 
 }  // extern "C"
