@@ -61,6 +61,11 @@ int sgb_ctx_destroy(sgb_ctx *ctx);
 int sgb_ctx_synchronize(sgb_ctx *ctx);
 const char *sgb_last_error(const sgb_ctx *ctx);
 const char *sgb_status_string(int status);
+/* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
+ * it instead of allocating, and releasing the batch does not free device memory (cudaFree
+ * synchronises the whole device, which would stall other contexts' work).  One batch at a time
+ * uses the arena; bytes = 0 releases it. */
+int sgb_ctx_reserve(sgb_ctx *ctx, size_t bytes);
 /* Bytes of device memory currently held by the context's molecules and batches. */
 size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
 

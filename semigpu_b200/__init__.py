@@ -38,6 +38,7 @@ SIGNATURES = {
     "sgb_last_error": (ctypes.c_char_p, [_VP]),
     "sgb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
+    "sgb_ctx_reserve": (ctypes.c_int, [_VP, ctypes.c_size_t]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
     "sgb_mol_destroy": (ctypes.c_int, [_VP]),
@@ -121,6 +122,10 @@ class Context:
 
     def synchronize(self):
         self.check(lib().sgb_ctx_synchronize(self.h), "synchronize")
+
+    def reserve(self, nbytes: int):
+        """Reusable device arena for batches of up to `nbytes` (see sgb_ctx_reserve)."""
+        self.check(lib().sgb_ctx_reserve(self.h, int(nbytes)), "sgb_ctx_reserve")
 
     @property
     def bytes_in_use(self) -> int:

@@ -62,6 +62,11 @@ struct sgb_ctx {
   cudaStream_t aux[kNumClasses] = {};
   cudaEvent_t joined[kNumClasses] = {};
   int class_threads[kNumClasses] = {};
+  // optional reusable arena (sgb_ctx_reserve): a batch that fits takes it instead of calling
+  // cudaMalloc, and gives it back without cudaFree (which would synchronise the device)
+  char* pool = nullptr;
+  size_t pool_bytes = 0;
+  bool pool_busy = false;
 };
 
 struct sgb_batch {
@@ -76,6 +81,7 @@ struct sgb_batch {
   int class_first[kNumClasses] = {}, class_count[kNumClasses] = {}, class_nmax[kNumClasses] = {};
   char* arena = nullptr;
   size_t bytes = 0;
+  bool from_pool = false;
   MolDesc* d_desc = nullptr;
   int* d_order = nullptr;
   int* d_counter = nullptr;
@@ -150,7 +156,9 @@ double cost_of(const MolDesc& d) { return (double)d.nao * d.nao * d.nao + 50.0 *
 
 void free_batch(sgb_batch* b) {
   if (!b) return;
-  if (b->arena) {
+  if (b->arena && b->from_pool) {
+    b->ctx->pool_busy = false;
+  } else if (b->arena) {
     cudaFree(b->arena);
     if (b->ctx) b->ctx->in_use -= b->bytes;
   }
@@ -249,17 +257,24 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
                o_stage = take(8 * (size_t)kStageSlots * nmol),
                o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0);
   b->bytes = off;
-  if (ctx->budget && ctx->in_use + off > ctx->budget) {
-    delete b;
-    return fail(ctx, SGB_E_NOMEM, "batch needs %zu bytes; budget %zu, in use %zu", off,
-                ctx->budget, ctx->in_use);
+  cudaError_t e = cudaSuccess;
+  if (ctx->pool && !ctx->pool_busy && off <= ctx->pool_bytes) {
+    b->arena = ctx->pool;
+    b->from_pool = true;
+    ctx->pool_busy = true;
+  } else {
+    if (ctx->budget && ctx->in_use + off > ctx->budget) {
+      delete b;
+      return fail(ctx, SGB_E_NOMEM, "batch needs %zu bytes; budget %zu, in use %zu", off,
+                  ctx->budget, ctx->in_use);
+    }
+    e = cudaMalloc(&b->arena, off);
+    if (e != cudaSuccess) {
+      delete b;
+      return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
+    }
+    ctx->in_use += off;
   }
-  cudaError_t e = cudaMalloc(&b->arena, off);
-  if (e != cudaSuccess) {
-    delete b;
-    return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
-  }
-  ctx->in_use += off;
   char* base = b->arena;
   b->d_desc = (MolDesc*)(base + o_desc);
   b->d_order = (int*)(base + o_order);
@@ -313,10 +328,18 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
 }
 
 // One kernel instantiation per (threads per CTA, eigenvector column registers per lane).
+// The dynamic shared memory cap is a per-function attribute shared by every host thread and
+// context, so it is always raised to the device's opt-in maximum (never to a launch's own size,
+// which another thread could lower between its set and its launch).
 template <int NT, int CR>
 cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStream_t st) {
   auto* k = k_batch_scf<NT, CR>;
-  cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (smem > (size_t)optin) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);
@@ -714,10 +737,35 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   return SGB_OK;
 }
 
+int sgb_ctx_reserve(sgb_ctx* ctx, size_t bytes) {
+  if (!ctx) return SGB_E_ARG;
+  if (ctx->pool_busy) return fail(ctx, SGB_E_STATE, "the reserved arena is in use by a batch");
+  if (ctx->pool) {
+    cudaFree(ctx->pool);
+    ctx->in_use -= ctx->pool_bytes;
+    ctx->pool = nullptr;
+    ctx->pool_bytes = 0;
+  }
+  if (!bytes) return SGB_OK;
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+    return fail(ctx, SGB_E_NOMEM, "reserve %zu bytes: budget %zu, in use %zu", bytes, ctx->budget,
+                ctx->in_use);
+  cudaError_t e = cudaMalloc(&ctx->pool, bytes);
+  if (e != cudaSuccess) {
+    ctx->pool = nullptr;
+    return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->pool_bytes = bytes;
+  ctx->in_use += bytes;
+  return SGB_OK;
+}
+
 int sgb_ctx_destroy(sgb_ctx* ctx) {
   if (!ctx) return SGB_E_ARG;
   cudaSetDevice(ctx->device);
   free_batch(ctx->cached);
+  ctx->cached = nullptr;
+  if (ctx->pool) cudaFree(ctx->pool);
   for (int k = 0; k < kNumClasses; ++k) {
     if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);

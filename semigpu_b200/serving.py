@@ -1,0 +1,192 @@
+"""Serving: molecules arrive one by one, results stream back, work overlaps on the device.
+
+A `Server` owns `slots` workers on one GPU.  Each worker has its own engine context (its own
+CUDA streams), so the persistent launches of different workers run concurrently on the device.
+A free worker takes every request waiting in the queue -- up to `max_batch` molecules and up to
+its share of the HBM budget, by each molecule's device footprint -- builds one device batch
+(integrals, Hcore, P, F, eigenvectors stay resident for the whole SCF) and runs it; requests
+that arrive meanwhile wait for the next free worker, so batches form continuously from whatever
+has arrived (continuous batching at launch granularity).  Molecules above the in-CTA size limit
+run through the single-molecule grid path in the worker that picked them.
+
+Latency of a request = completion time - arrival time (host clock); `stats()` reports p50/p99
+and throughput.  `replay()` drives an open-loop arrival schedule (e.g. Poisson) in real time.
+"""
+from __future__ import annotations
+
+import collections
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import Context, Molecule, run_molecules
+from .geometry import Molecule as Geometry
+
+CTA_MAX_NAO = 160  # larger molecules take the grid path
+
+
+def device_bytes(mol: Geometry) -> int:
+    """Device memory a molecule occupies inside a batch (integral blocks, Hcore/P/F packed,
+    eigenvectors + F full square, eigenvalues, atom arrays)."""
+    heavy = int(np.count_nonzero(mol.Z > 1))
+    light = mol.natoms - heavy
+    nblk = 100 * heavy * (heavy + 1) // 2 + 10 * heavy * light + light * (light + 1) // 2
+    n = mol.nao
+    return 8 * (nblk + 3 * n * (n + 1) // 2 + 2 * n * n + n) + 64 * mol.natoms + 256
+
+
+@dataclass
+class Request:
+    rid: int
+    mol: Geometry
+    t_arrival: float
+    t_start: float = 0.0
+    t_done: float = 0.0
+    result: dict = field(default_factory=dict)
+
+
+class Server:
+    def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
+                 hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
+                 batch_window_s: float = 0.0, engine=None):
+        """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
+        replaceable for host-only tests of the scheduling."""
+        self.tol, self.max_iter = tol, max_iter
+        self.max_batch = max_batch
+        self.slot_budget = hbm_budget // max(1, slots)
+        self.window = batch_window_s
+        self.engine = engine or run_molecules
+        self._queue: collections.deque[Request] = collections.deque()
+        self._cv = threading.Condition()
+        self._done: list[Request] = []
+        self._next = 0
+        self._stop = False
+        self._device = device
+        self._workers = [threading.Thread(target=self._work, args=(i,), daemon=True)
+                         for i in range(slots)]
+        self.batches: list[tuple[int, int, float, float]] = []  # (worker, size, t0, t1)
+        self._errors: list[BaseException] = []
+        for w in self._workers:
+            w.start()
+
+    # -- client side -----------------------------------------------------------------------
+    def submit(self, mol: Geometry, t_arrival: float | None = None) -> int:
+        with self._cv:
+            rid = self._next
+            self._next += 1
+            self._queue.append(Request(rid, mol, time.perf_counter() if t_arrival is None else t_arrival))
+            self._cv.notify()
+        return rid
+
+    def drain(self, timeout: float = 600.0) -> list[Request]:
+        """Waits until every submitted request has completed; returns them by request id."""
+        t_end = time.perf_counter() + timeout
+        with self._cv:
+            while len(self._done) < self._next:
+                if self._errors:
+                    raise self._errors[0]
+                left = t_end - time.perf_counter()
+                if left <= 0:
+                    raise TimeoutError(f"{self._next - len(self._done)} requests unfinished")
+                self._cv.wait(min(left, 0.05))
+            return sorted(self._done, key=lambda r: r.rid)
+
+    def close(self):
+        with self._cv:
+            self._stop = True
+            self._cv.notify_all()
+        for w in self._workers:
+            w.join(timeout=60)
+
+    def replay(self, arrivals, time_scale: float = 1.0) -> list[Request]:
+        """Submits (t, molecule) pairs at their arrival times (open loop) and waits for all."""
+        t0 = time.perf_counter()
+        for t, mol in arrivals:
+            delay = t0 + t * time_scale - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            self.submit(mol, t_arrival=t0 + t * time_scale)
+        return self.drain()
+
+    # -- worker side ------------------------------------------------------------------------
+    def _take(self) -> list[Request]:
+        """Everything waiting, up to max_batch molecules and this worker's HBM share."""
+        out, used = [], 0
+        while self._queue and len(out) < self.max_batch:
+            need = device_bytes(self._queue[0].mol)
+            if out and used + need > self.slot_budget:
+                break
+            used += need
+            out.append(self._queue.popleft())
+        return out
+
+    def _work(self, idx: int):
+        ctx = None
+        try:
+            if self.engine is run_molecules:
+                ctx = Context(self._device)
+                # batches are built in a per-worker arena: no cudaMalloc/cudaFree per batch
+                # (cudaFree would synchronise the device and stall the other workers)
+                ctx.reserve(self.slot_budget + (64 << 20))
+            while True:
+                with self._cv:
+                    while not self._queue and not self._stop:
+                        self._cv.wait(0.05)
+                    if self._stop and not self._queue:
+                        return
+                if self.window:
+                    time.sleep(self.window)
+                with self._cv:
+                    reqs = self._take()
+                if not reqs:
+                    continue
+                t0 = time.perf_counter()
+                for r in reqs:
+                    r.t_start = t0
+                small = [r for r in reqs if r.mol.nao <= CTA_MAX_NAO]
+                large = [r for r in reqs if r.mol.nao > CTA_MAX_NAO]
+                if small:
+                    res = self.engine(ctx, [r.mol for r in small], self.tol, self.max_iter)
+                    t1 = time.perf_counter()
+                    for j, r in enumerate(small):
+                        r.result = {k: (v[j].item() if hasattr(v[j], "item") else v[j])
+                                    for k, v in res.items()}
+                        r.t_done = t1
+                for r in large:
+                    if self.engine is run_molecules:
+                        m = Molecule.from_geometry(ctx, r.mol)
+                        res = m.run(tol=self.tol, max_iter=self.max_iter)
+                        m.close()
+                        r.result = {k: res[k] for k in ("E_el", "E_cc", "E_tot", "n_iter",
+                                                        "converged", "status")}
+                    else:
+                        res = self.engine(ctx, [r.mol], self.tol, self.max_iter)
+                        r.result = {k: (v[0].item() if hasattr(v[0], "item") else v[0])
+                                    for k, v in res.items()}
+                    r.t_done = time.perf_counter()
+                with self._cv:
+                    self.batches.append((idx, len(reqs), t0, time.perf_counter()))
+                    self._done.extend(reqs)
+                    self._cv.notify_all()
+        except BaseException as exc:  # surfaced to drain()
+            with self._cv:
+                self._errors.append(exc)
+                self._cv.notify_all()
+        finally:
+            if ctx is not None:
+                ctx.close()
+
+
+def stats(done: list[Request]) -> dict:
+    """p50/p99 time-to-converged-energy (arrival -> result) and throughput."""
+    if not done:
+        return {}
+    lat = np.array([r.t_done - r.t_arrival for r in done])
+    t_first = min(r.t_arrival for r in done)
+    t_last = max(r.t_done for r in done)
+    return {"requests": len(done), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+            "molecules_per_s": len(done) / (t_last - t_first) if t_last > t_first else float("nan"),
+            "all_converged": bool(all(r.result.get("converged", False) for r in done))}

@@ -1,0 +1,90 @@
+"""Serving scheduler (host logic) with a stand-in engine, and the real engine on the GPU."""
+from __future__ import annotations
+
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from semigpu_b200 import geometry as geo
+from semigpu_b200 import serving
+
+
+def _fake_engine(delay=0.002, log=None):
+    lock = threading.Lock()
+
+    def run(ctx, mols, tol, max_iter):
+        with lock:
+            if log is not None:
+                log.append(len(mols))
+        time.sleep(delay)
+        n = len(mols)
+        return {"E_el": np.array([-float(m.nao) for m in mols]), "E_cc": np.zeros(n),
+                "E_tot": np.array([-float(m.nao) for m in mols]), "n_iter": np.ones(n, np.int32),
+                "converged": np.ones(n, bool), "status": np.zeros(n, np.int32)}
+    return run
+
+
+def test_every_request_answered_once_with_its_own_result():
+    log = []
+    srv = serving.Server(slots=3, engine=_fake_engine(log=log))
+    try:
+        mols = geo.batch_c3(300, seed=2)
+        ids = [srv.submit(m) for m in mols]
+        done = srv.drain(timeout=60)
+    finally:
+        srv.close()
+    assert [r.rid for r in done] == ids
+    for r, m in zip(done, mols):
+        assert r.result["E_el"] == -float(m.nao)
+        assert r.t_done >= r.t_arrival
+    assert sum(log) == 300
+    assert len(log) < 300  # requests were batched
+
+
+def test_admission_respects_hbm_share():
+    log = []
+    mols = geo.batch_c3(50, seed=3)
+    biggest = max(serving.device_bytes(m) for m in mols)
+    srv = serving.Server(slots=1, hbm_budget=3 * biggest, engine=_fake_engine(delay=0.01, log=log))
+    try:
+        for m in mols:
+            srv.submit(m)
+        srv.drain(timeout=60)
+    finally:
+        srv.close()
+    assert max(log) <= 50 and len(log) > 1
+
+
+def test_open_loop_replay_and_stats():
+    srv = serving.Server(slots=2, engine=_fake_engine(delay=0.001))
+    try:
+        arrivals = serving_arrivals = [(0.001 * i, m) for i, m in enumerate(geo.batch_c3(60, seed=5))]
+        done = srv.replay(serving_arrivals)
+    finally:
+        srv.close()
+    s = serving.stats(done)
+    assert s["requests"] == 60 and s["p99_ms"] >= s["p50_ms"] > 0 and s["all_converged"]
+
+
+@pytest.mark.gpu
+def test_served_results_equal_alone():
+    """Each molecule gives the same energy served in a mixed stream as computed alone."""
+    import semigpu_b200 as sg
+
+    mols = geo.batch_c3(96, seed=21)
+    srv = serving.Server(slots=3, hbm_budget=2 << 30)
+    try:
+        arrivals = [(0.0005 * i, m) for i, m in enumerate(mols)]
+        done = srv.replay(arrivals)
+    finally:
+        srv.close()
+    assert len(done) == 96 and all(r.result["status"] == 0 for r in done)
+    with sg.Context(0) as ctx:
+        for i in (0, 13, 50, 95):
+            alone = sg.Molecule.from_geometry(ctx, mols[i]).run(tol=1e-6)
+            assert done[i].result["n_iter"] == alone["n_iter"]
+            assert abs(done[i].result["E_tot"] - alone["E_tot"]) < 1e-9
+    s = serving.stats(done)
+    assert s["all_converged"] and s["p99_ms"] > 0
