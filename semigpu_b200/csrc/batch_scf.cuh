@@ -99,12 +99,12 @@ constexpr int kVsmemMax = 110;  // 2 * 110 * 111 doubles = 195 KB: G and V both 
 constexpr double kJacobiRotAbs = 1e-12;
 constexpr double kJacobiDoneAbs = 1e-7;
 
-// The first kFullJacobiSteps eigensolves of an SCF rotate every pair (the occupied set is still
-// moving).  Later ones rotate occupied-virtual pairs only and are accepted when the largest
+// The first eigensolve of an SCF (no previous vectors) rotates every pair.  Later ones rotate
+// occupied-virtual pairs only and are accepted when the largest
 // occupied Rayleigh quotient stays kCrossMargin eV below the smallest virtual one (the
 // quotients differ from eigenvalues by the small within-block couplings left unrotated);
 // otherwise a full Jacobi follows, so the occupied set is always the nocc lowest states.
-constexpr int kFullJacobiSteps = 3;
+constexpr int kFullJacobiSteps = 1;
 constexpr double kCrossMargin = 1.0;
 // Occupied-virtual couplings sit across a gap of at least kCrossMargin, where Jacobi converges
 // quadratically: after a sweep whose largest coupling was below kJacobiDoneGapped the next
@@ -199,16 +199,18 @@ __device__ inline void split_by_rank(const double* dval, int n, int nocc, int* o
   }
 }
 
-template <int NT, int CR>
+// V_SMEM: the eigenvectors live in shared memory next to G (nao <= kVsmemMax) rather than in
+// global memory; a template parameter so every access in the eigensolver has a known address
+// space.
+template <int NT, int CR, bool V_SMEM>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
   const MolView m = make_view(a, d);
   const int n = m.nao, ld = smem_ld(n);
   const size_t nmax = (size_t)a.nmax;
-  const bool v_smem = mat_doubles_for(n) == 2 * (size_t)n * ld;
   double* G = smem;
-  double* V = v_smem ? smem + (size_t)n * ld : m.V;
-  const int ldv = v_smem ? ld : n;
+  double* V = V_SMEM ? smem + (size_t)n * ld : m.V;
+  const int ldv = V_SMEM ? ld : n;
   double* wq = smem + a.mat_doubles;
   double* dval = wq + 3 * nmax + 8;
   double* red = dval + nmax;
@@ -356,7 +358,11 @@ __global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
     const int q = s_next;
     __syncthreads();
     if (q >= a.nmol) break;
-    run_molecule<NT, CR>(a, a.order[q], smem);
+    const int mi = a.order[q];
+    if (mat_doubles_for(a.mols[mi].nao) == 2 * (size_t)a.mols[mi].nao * smem_ld(a.mols[mi].nao))
+      run_molecule<NT, CR, true>(a, mi, smem);
+    else
+      run_molecule<NT, CR, false>(a, mi, smem);
   }
 }
 

@@ -337,9 +337,12 @@ cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStre
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
   if (e != cudaSuccess) return e;
-  if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  const int max_dynamic = optin - (int)fa.sharedSizeBytes;  // the static part counts against it
+  if (smem > (size_t)max_dynamic) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);

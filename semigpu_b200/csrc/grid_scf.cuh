@@ -344,13 +344,7 @@ __global__ void __launch_bounds__(256) k_grid_jacobi(GridJacobiArgs a) {
           apq = fma(xv, yg, apq);
           aqp = fma(xg, yv, aqp);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          app += __shfl_xor_sync(0xffffffffu, app, o);
-          aqq += __shfl_xor_sync(0xffffffffu, aqq, o);
-          apq += __shfl_xor_sync(0xffffffffu, apq, o);
-          aqp += __shfl_xor_sync(0xffffffffu, aqp, o);
-        }
+        warp_sum4(lane, app, aqq, apq, aqp);
         const double a_pq = 0.5 * (apq + aqp);
         if (!(fabs(a_pq) > a.rot_abs)) {
           if (a_pq != a_pq) worst = INFINITY;

@@ -360,6 +360,28 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Warp sums of four values, every lane receiving all four.  The first two butterfly levels
+// split the values between lane halves (each lane forwards the sums it does not keep), so the
+// reduction costs 6 exchanges plus 4 broadcasts instead of 4 x 5 exchanges.
+__device__ __forceinline__ void warp_sum4(int lane, double& a, double& b, double& c, double& d) {
+  const bool hi16 = lane & 16, hi8 = lane & 8;
+  // level 16: lower half keeps (a, b), upper half keeps (c, d)
+  double x = __shfl_xor_sync(0xffffffffu, hi16 ? a : c, 16);
+  double y = __shfl_xor_sync(0xffffffffu, hi16 ? b : d, 16);
+  double k0 = (hi16 ? c : a) + x;
+  double k1 = (hi16 ? d : b) + y;
+  // level 8: lanes with bit 3 clear keep k0, set keep k1
+  const double z = __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
+  double v = (hi8 ? k1 : k0) + z;
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  // lane 0 holds a, lane 8 b, lane 16 c, lane 24 d
+  a = __shfl_sync(0xffffffffu, v, 0);
+  b = __shfl_sync(0xffffffffu, v, 8);
+  c = __shfl_sync(0xffffffffu, v, 16);
+  d = __shfl_sync(0xffffffffu, v, 24);
+}
+
 // Shift making F + mu I positive semi-definite: mu = ||F||_inf + 1 (row sums of |F_ij|).
 template <int NT>
 __device__ double block_shift(int n, const double* Ffull, double* red) {
@@ -441,7 +463,9 @@ __device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
 // grp_b (nb entries, na <= nb) are rotated -- round r pairs grp_a[k] with grp_b[(k + r) % nb],
 // nb rounds per sweep.  The SCF uses it with the occupied and virtual columns: the density
 // matrix only depends on the occupied subspace, which these rotations alone decide.
-template <int NT, int CR>
+// Each warp carries PP column pairs of a round at once (independent dependency chains
+// interleaved), which hides the latency of the dot-product reduction and the angle computation.
+template <int NT, int CR, int PP = 2>
 __device__ int block_jacobi_fv(int n, double* G, int ldg, double* V, int ldv, double* red,
                                double rot_abs, double done_abs, int max_sweeps,
                                const int* grp_a = nullptr, int na = 0, const int* grp_b = nullptr,
@@ -454,67 +478,90 @@ __device__ int block_jacobi_fv(int n, double* G, int ldg, double* V, int ldv, do
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double worst = 0.0;
     for (int r = 0; r < rounds; ++r) {
-      for (int k = warp; k < per_round; k += NW) {
-        int p, q;
-        if (bip) {
-          p = grp_a[k];
-          int j = k + r;
-          if (j >= nb) j -= nb;
-          q = grp_b[j];
-        } else {
-          rr_pair(r, k, m, p, q);
-          if (p >= n || q >= n) continue;
-        }
-        double* gp = G + (int64_t)p * ldg;
-        double* gq = G + (int64_t)q * ldg;
-        double* vp = V + (int64_t)p * ldv;
-        double* vq = V + (int64_t)q * ldv;
-        double xg[CR], yg[CR], xv[CR], yv[CR];
-        double app = 0.0, aqq = 0.0, apq = 0.0, aqp = 0.0;
+      for (int k0 = warp; k0 < per_round; k0 += PP * NW) {
+        int p[PP], q[PP];
+        bool live[PP];
 #pragma unroll
-        for (int j = 0; j < CR; ++j) {
-          const int i = lane + 32 * j;
-          const bool in = i < n;
-          xg[j] = in ? gp[i] : 0.0;
-          yg[j] = in ? gq[i] : 0.0;
-          xv[j] = in ? vp[i] : 0.0;
-          yv[j] = in ? vq[i] : 0.0;
+        for (int u = 0; u < PP; ++u) {
+          const int k = k0 + u * NW;
+          live[u] = k < per_round;
+          p[u] = 0;
+          q[u] = 0;
+          if (live[u]) {
+            if (bip) {
+              p[u] = grp_a[k];
+              int j = k + r;
+              if (j >= nb) j -= nb;
+              q[u] = grp_b[j];
+            } else {
+              rr_pair(r, k, m, p[u], q[u]);
+              live[u] = p[u] < n && q[u] < n;
+              if (!live[u]) p[u] = q[u] = 0;
+            }
+          }
+        }
+        double xg[PP][CR], yg[PP][CR], xv[PP][CR], yv[PP][CR];
+        double app[PP], aqq[PP], apq[PP], aqp[PP];
+#pragma unroll
+        for (int u = 0; u < PP; ++u) {
+          const double* gp = G + (int64_t)p[u] * ldg;
+          const double* gq = G + (int64_t)q[u] * ldg;
+          const double* vp = V + (int64_t)p[u] * ldv;
+          const double* vq = V + (int64_t)q[u] * ldv;
+#pragma unroll
+          for (int j = 0; j < CR; ++j) {
+            const int i = lane + 32 * j;
+            const bool in = live[u] && i < n;
+            xg[u][j] = in ? gp[i] : 0.0;
+            yg[u][j] = in ? gq[i] : 0.0;
+            xv[u][j] = in ? vp[i] : 0.0;
+            yv[u][j] = in ? vq[i] : 0.0;
+          }
         }
 #pragma unroll
-        for (int j = 0; j < CR; ++j) {
-          app = fma(xv[j], xg[j], app);
-          aqq = fma(yv[j], yg[j], aqq);
-          apq = fma(xv[j], yg[j], apq);
-          aqp = fma(xg[j], yv[j], aqp);
+        for (int u = 0; u < PP; ++u) {
+          app[u] = aqq[u] = apq[u] = aqp[u] = 0.0;
+#pragma unroll
+          for (int j = 0; j < CR; ++j) {
+            app[u] = fma(xv[u][j], xg[u][j], app[u]);
+            aqq[u] = fma(yv[u][j], yg[u][j], aqq[u]);
+            apq[u] = fma(xv[u][j], yg[u][j], apq[u]);
+            aqp[u] = fma(xg[u][j], yv[u][j], aqp[u]);
+          }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          app += __shfl_xor_sync(0xffffffffu, app, o);
-          aqq += __shfl_xor_sync(0xffffffffu, aqq, o);
-          apq += __shfl_xor_sync(0xffffffffu, apq, o);
-          aqp += __shfl_xor_sync(0xffffffffu, aqp, o);
-        }
-        const double a_pq = 0.5 * (apq + aqp);
-        if (!(fabs(a_pq) > rot_abs)) {
-          if (a_pq != a_pq) worst = INFINITY;
-          continue;
-        }
-        worst = fmax(worst, fabs(a_pq));
-        // tan of the angle zeroing A_pq: t = sgn(den) num / (|den| + hypot(den, num)),
-        // num = 2 A_pq, den = A_qq - A_pp (the smaller of the two roots)
-        const float num = (float)(2.0 * a_pq), den = (float)(aqq - app);
-        float tf = num / (fabsf(den) + hypotf(den, num));
-        if (den < 0.0f) tf = -tf;
-        const double t = (double)tf;
-        const double c = rsqrt(fma(t, t, 1.0)), s = c * t;
+        for (int u = 0; u < PP; ++u) warp_sum4(lane, app[u], aqq[u], apq[u], aqp[u]);
 #pragma unroll
-        for (int j = 0; j < CR; ++j) {
-          const int i = lane + 32 * j;
-          if (i < n) {
-            gp[i] = c * xg[j] - s * yg[j];
-            gq[i] = s * xg[j] + c * yg[j];
-            vp[i] = c * xv[j] - s * yv[j];
-            vq[i] = s * xv[j] + c * yv[j];
+        for (int u = 0; u < PP; ++u) {
+          const double a_pq = 0.5 * (apq[u] + aqp[u]);
+          if (!live[u]) continue;
+          if (!(fabs(a_pq) > rot_abs)) {
+            if (a_pq != a_pq) worst = INFINITY;
+            continue;
+          }
+          worst = fmax(worst, fabs(a_pq));
+          // tan of the angle zeroing A_pq: t = sgn(den) num / (|den| + hypot(den, num)),
+          // num = 2 A_pq, den = A_qq - A_pp (the smaller of the two roots)
+          // approximate FP32 arithmetic is enough here: the angle may be slightly off, the
+          // rotation applied below is exactly orthogonal
+          const float num = (float)(2.0 * a_pq), den = (float)(aqq[u] - app[u]);
+          float tf = __fdividef(num, fabsf(den) + __fsqrt_rn(fmaf(den, den, num * num)));
+          if (den < 0.0f) tf = -tf;
+          const double t = (double)tf;
+          const double c = rsqrt(fma(t, t, 1.0)), sn = c * t;
+          double* gp = G + (int64_t)p[u] * ldg;
+          double* gq = G + (int64_t)q[u] * ldg;
+          double* vp = V + (int64_t)p[u] * ldv;
+          double* vq = V + (int64_t)q[u] * ldv;
+#pragma unroll
+          for (int j = 0; j < CR; ++j) {
+            const int i = lane + 32 * j;
+            if (i < n) {
+              gp[i] = c * xg[u][j] - sn * yg[u][j];
+              gq[i] = sn * xg[u][j] + c * yg[u][j];
+              vp[i] = c * xv[u][j] - sn * yv[u][j];
+              vq[i] = sn * xv[u][j] + c * yv[u][j];
+            }
           }
         }
       }
