@@ -348,6 +348,28 @@ def run_ours(args):
             sg.Molecule.from_geometry(ctx, m).run(tol=TOL)
             plain_lat.append(time.perf_counter() - t1)
         plain = len(sample) / (time.perf_counter() - tp)
+        # serving: open-loop Poisson arrivals of the same composition, continuous batching over
+        # three worker contexts (semigpu_b200.serving); warmed up first
+        from semigpu_b200 import serving
+
+        srate, sdur = 2000.0, 3.0
+        srng = np.random.default_rng(11)
+        smols = geo.batch_c3(int(srate * sdur * 1.3) + 64, seed=1000 + rank)
+        arrivals, t_a = [], 0.0
+        while True:
+            t_a += srng.exponential(1.0 / srate)
+            if t_a >= sdur:
+                break
+            arrivals.append((t_a, smols[len(arrivals)]))
+        srv = serving.Server(device=local, slots=3, hbm_budget=12 << 30, tol=TOL)
+        try:
+            srv.replay([(0.001 * i, m) for i, m in enumerate(smols[-64:])])  # warm-up
+            srv_done = srv.replay(arrivals)
+        finally:
+            srv.close()
+        served = serving.stats(srv_done)
+        served.update({"rate_per_s": srate, "duration_s": sdur, "slots": 3,
+                       "composition": "as the batch (seeded), open-loop Poisson arrivals"})
         # CPU baseline: the reference build on the host cores, bounded sample
         cpu = None
         if reference_kind():
@@ -377,6 +399,7 @@ def run_ours(args):
                                "sample": "48 molecules stratified by nao, one molecule per call "
                                          "through the stage API"},
             "speedup_vs_plain_fp64_gpu": value / plain,
+            "serving": served,
             "all_converged": ok,
             "roofline": roof,
             "cpu_baseline": cpu,

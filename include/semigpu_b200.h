@@ -93,6 +93,11 @@ size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
 #define SGB_P_EISOL 17
 #define SGB_PARAM_COUNT 18
 int sgb_mndo_parameters(int Z, double *values);
+/* Heat of formation (kcal/mol) from a total energy (eV, electronic + core-core), MOPAC's
+ * convention: (E_tot - sum_A E_isol(A)) * 23.060548 + sum_A dH_f(atom A), with the atomic
+ * E_isol ("eisol") and dH_f ("heat") of MNDO_parameters.cpp:47-122, which the reference stores
+ * but never uses.  Host arithmetic only; no counterpart in the reference's SCF path. */
+int sgb_heat_of_formation(int natoms, const int *Z, double e_tot, double *dhf_kcal);
 
 /* ---- one molecule: the reference's stage API ------------------------------------------- */
 /* Replaces ReadXYZFile output handling + ListAtomicOrbitals::SetOrbitals

@@ -40,6 +40,7 @@ SIGNATURES = {
     "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
     "sgb_ctx_reserve": (ctypes.c_int, [_VP, ctypes.c_size_t]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
+    "sgb_heat_of_formation": (ctypes.c_int, [ctypes.c_int, _I, ctypes.c_double, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
     "sgb_mol_destroy": (ctypes.c_int, [_VP]),
     "sgb_mol_info": (ctypes.c_int, [_VP, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
@@ -97,6 +98,25 @@ def _d(a):
 
 def _i(a):
     return a.ctypes.data_as(_I)
+
+
+def heat_of_formation(Z, e_tot: float) -> float:
+    """kcal/mol from the total energy in eV (MOPAC convention, atomic eisol / heat data)."""
+    Z = np.ascontiguousarray(Z, np.int32)
+    out = ctypes.c_double()
+    rc = lib().sgb_heat_of_formation(len(Z), _i(Z), float(e_tot), ctypes.byref(out))
+    if rc:
+        raise SGBError(rc, lib().sgb_status_string(rc).decode())
+    return out.value
+
+
+def mndo_parameters(z: int) -> np.ndarray:
+    """The engine's MNDO parameters of element z (order of the SGB_P_* indices)."""
+    out = np.zeros(18)
+    rc = lib().sgb_mndo_parameters(int(z), _d(out))
+    if rc:
+        raise SGBError(rc, lib().sgb_status_string(rc).decode())
+    return out
 
 
 class _ScfResult(ctypes.Structure):
@@ -214,6 +234,7 @@ class Molecule:
         r = self.scf(tol, max_iter)
         r["E_cc"] = self.core_core()
         r["E_tot"] = r["E_el"] + r["E_cc"]
+        r["dHf_kcal"] = heat_of_formation(self.Z, r["E_tot"])
         return r
 
     def close(self):

@@ -682,6 +682,20 @@ const char* sgb_status_string(int s) {
 
 const char* sgb_last_error(const sgb_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+int sgb_heat_of_formation(int natoms, const int* Z, double e_tot, double* dhf) {
+  if (natoms <= 0 || !Z || !dhf) return SGB_E_ARG;
+  constexpr double kEvToKcal = 23.060548;  // kcal/mol per eV (CODATA 2018)
+  double eisol = 0.0, heat = 0.0;
+  for (int a = 0; a < natoms; ++a) {
+    double v[SGB_PARAM_COUNT];
+    if (sgb_mndo_parameters(Z[a], v) != SGB_OK) return SGB_E_ELEMENT;
+    eisol += v[SGB_P_EISOL];
+    heat += v[SGB_P_HEAT];
+  }
+  *dhf = (e_tot - eisol) * kEvToKcal + heat;
+  return SGB_OK;
+}
+
 int sgb_mndo_parameters(int Z, double* v) {
   const int s = slot_of(Z);
   if (s < 0 || !v) return SGB_E_ELEMENT;

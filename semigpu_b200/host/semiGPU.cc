@@ -3,6 +3,7 @@
 // as in the reference; optional flags before it:
 //   --tol T       SCF energy threshold in eV (default 5e-3, the reference's hard-coded value)
 //   --max-iter M  SCF step cap (default 100)
+//   --heat        also print the heat of formation (not printed by the reference)
 #include <chrono>
 #include <cstdlib>
 #include <cstring>
@@ -11,6 +12,7 @@
 #include <vector>
 
 #include "semigpu.h"
+#include "semigpu_b200.h"
 
 using std::cout;
 using std::endl;
@@ -24,9 +26,11 @@ int main(int argc, char* argv[]) {
   }
   double tol = 5.0e-3;
   unsigned max_iter = 100;
+  bool heat = false;
   for (int a = 1; a + 1 < argc; ++a) {
     if (!strcmp(argv[a], "--tol")) tol = atof(argv[++a]);
     else if (!strcmp(argv[a], "--max-iter")) max_iter = (unsigned)atoi(argv[++a]);
+    else if (!strcmp(argv[a], "--heat")) heat = true;
   }
   string filename_molecule = argv[argc - 1];
   cout << "XYZ file : " << filename_molecule << endl;
@@ -94,6 +98,13 @@ int main(int argc, char* argv[]) {
   cout << "       Total Energy = " << setw(10) << electronicEnergy + coreCoreRepulsionEnergy
        << " eV" << endl;
   ScreenUtils::PrintScrStarLine();
+  if (heat) {
+    double dhf = 0.0;
+    sgb_heat_of_formation((int)infoAOs.Z.size(), infoAOs.Z.data(),
+                          electronicEnergy + coreCoreRepulsionEnergy, &dhf);
+    cout << "  Heat of Formation = " << setw(10) << dhf << " kcal/mol" << endl;
+    ScreenUtils::PrintScrStarLine();
+  }
 
   cout << "Dealloc array: SCFData" << endl;
   SCFprocess.DeallocSCFData();
