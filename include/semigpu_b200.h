@@ -109,7 +109,8 @@ int sgb_mol_create(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, sg
 int sgb_mol_destroy(sgb_mol *mol);
 /* Execution path of the stage calls: AUTO picks one CTA per molecule with its SCF matrices in
  * shared memory for nao <= 160 and the grid-wide kernels (host-driven SCF loop, cooperative
- * Jacobi) above that; CTA / GRID force one (CTA refuses SCF above nao 160). */
+ * Jacobi) above that; CTA / GRID force one (CTA streams its eigensolver matrices from global
+ * memory above nao 160 and refuses SCF above nao 1024). */
 #define SGB_PATH_AUTO 0
 #define SGB_PATH_CTA 1
 #define SGB_PATH_GRID 2
@@ -146,7 +147,8 @@ int sgb_batch_destroy(sgb_batch *b);
 /* Replaces new coordinates for the same molecules (same atom counts and elements): one
  * host->device copy of natoms_total*3 doubles. */
 int sgb_batch_set_coordinates(sgb_ctx *ctx, sgb_batch *b, const double *xyz);
-/* Integrals, Hcore, SCF and core-core repulsion of every molecule, one persistent launch. */
+/* Integrals, Hcore, SCF and core-core repulsion of every molecule, one persistent launch per
+ * size class; one CTA per molecule, nao <= 1024 (larger: SGB_E_UNSUPPORTED, use sgb_scf). */
 int sgb_batch_run(sgb_ctx *ctx, sgb_batch *b, double tol, int max_iter);
 /* Per-molecule results (any pointer may be NULL).  Blocks until the run has finished. */
 int sgb_batch_results(sgb_ctx *ctx, sgb_batch *b, double *e_el, double *e_cc, int *n_iter,

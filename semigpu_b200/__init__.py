@@ -190,7 +190,7 @@ class Molecule:
         return cls(ctx, mol.Z, mol.xyz)
 
     def set_path(self, path: int):
-        """PATH_AUTO, PATH_CTA (one CTA per molecule, nao <= 160) or PATH_GRID (whole GPU)."""
+        """PATH_AUTO, PATH_CTA (one CTA per molecule, nao <= 1024) or PATH_GRID (whole GPU)."""
         self.ctx.check(lib().sgb_mol_set_path(self.h, path), "sgb_mol_set_path")
 
     def two_center(self):

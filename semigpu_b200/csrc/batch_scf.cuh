@@ -35,6 +35,7 @@ struct BatchArgs {
   double* V;
   double* T;
   double* eig;
+  double* W;        // eigensolver work matrices of the molecules above nao 160
   double* e_el;
   double* e_cc;
   int* n_iter;
@@ -111,8 +112,12 @@ constexpr double kCrossMargin = 1.0;
 // would start below n * 3e-6^2 / 1 eV ~ 1e-9 eV (n <= 160), so no confirmation sweep is run.
 constexpr double kJacobiDoneGapped = 3e-6;
 
+// Largest nao whose G fits one CTA's shared memory; above it G and V are global (streamed).
+constexpr int kGsmemMax = 160;
+
 __host__ __device__ inline size_t mat_doubles_for(int n) {
   const size_t ld = (size_t)smem_ld(n);
+  if (n > kGsmemMax) return 0;
   return (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
 }
 
@@ -135,6 +140,7 @@ __device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& 
   v.H = a.H + d.pk0; v.P = a.P + d.pk0; v.F = a.F + d.pk0;
   v.V = a.V + d.sq0; v.T = a.T + d.sq0;
   v.eig = a.eig + d.ao0;
+  v.W = a.W ? a.W + d.w0 : nullptr;
   return v;
 }
 
@@ -199,18 +205,18 @@ __device__ inline void split_by_rank(const double* dval, int n, int nocc, int* o
   }
 }
 
-// V_SMEM: the eigenvectors live in shared memory next to G (nao <= kVsmemMax) rather than in
-// global memory; a template parameter so every access in the eigensolver has a known address
-// space.
-template <int NT, int CR, bool V_SMEM>
+// PLACE: 0 = G and V in shared memory (nao <= kVsmemMax), 1 = G in shared memory and V in
+// global memory (nao <= kGsmemMax), 2 = both in global memory (larger; CR must be 0).  A
+// template parameter so every access in the eigensolver has a known address space.
+template <int NT, int CR, int PLACE>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
   const MolView m = make_view(a, d);
-  const int n = m.nao, ld = smem_ld(n);
+  const int n = m.nao, ld = PLACE == 2 ? n : smem_ld(n);
   const size_t nmax = (size_t)a.nmax;
-  double* G = smem;
-  double* V = V_SMEM ? smem + (size_t)n * ld : m.V;
-  const int ldv = V_SMEM ? ld : n;
+  double* G = PLACE == 2 ? m.W : smem;
+  double* V = PLACE == 0 ? smem + (size_t)n * ld : m.V;
+  const int ldv = PLACE == 0 ? ld : n;
   double* wq = smem + a.mat_doubles;
   double* dval = wq + 3 * nmax + 8;
   double* red = dval + nmax;
@@ -359,10 +365,15 @@ __global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
     __syncthreads();
     if (q >= a.nmol) break;
     const int mi = a.order[q];
-    if (mat_doubles_for(a.mols[mi].nao) == 2 * (size_t)a.mols[mi].nao * smem_ld(a.mols[mi].nao))
-      run_molecule<NT, CR, true>(a, mi, smem);
-    else
-      run_molecule<NT, CR, false>(a, mi, smem);
+    const int n = a.mols[mi].nao;
+    if constexpr (CR == 0) {
+      run_molecule<NT, 0, 2>(a, mi, smem);
+    } else {
+      if (n <= kVsmemMax)
+        run_molecule<NT, CR, 0>(a, mi, smem);
+      else
+        run_molecule<NT, CR, 1>(a, mi, smem);
+    }
   }
 }
 

@@ -25,14 +25,17 @@ namespace {
 constexpr int kSmallNmax = 160;  // largest nao whose n x n FP64 matrix fits one CTA's smem
 
 // Size classes of the batched launch, by nao: (upper bound, eigenvector column registers per
-// lane, default threads per CTA).  The last class holds molecules too large for the in-CTA
-// SCF; only the integral, Hcore, Fock and core-core stages run there.
+// lane, default threads per CTA).  Up to nao 160 the eigensolver's columns sit in registers
+// and shared memory; the class up to 1024 streams them from global memory (CR 0).  The last
+// class holds molecules too large for one CTA's SCF; only the integral, Hcore, Fock and
+// core-core stages run there (their SCF is the grid path of sgb_scf).
 struct SizeClass {
   int nmax, cr, threads;
 };
-constexpr SizeClass kClasses[] = {{64, 2, 512}, {96, 3, 512}, {128, 4, 512}, {160, 5, 512},
-                                  {1 << 30, 2, 512}};
-constexpr int kNumClasses = 5;
+constexpr SizeClass kClasses[] = {{64, 2, 512},   {96, 3, 512},        {128, 4, 512}, {160, 5, 512},
+                                  {1024, 0, 512}, {1 << 30, 0, 512}};
+constexpr int kNumClasses = 6;
+constexpr int kBatchScfMax = 1024;  // one CTA per molecule up to here; the grid path above
 
 int class_of(int nao) {
   int c = 0;
@@ -92,7 +95,7 @@ struct sgb_batch {
   int64_t* d_row_off = nullptr;
   int* d_hb = nullptr;
   double *d_ints = nullptr, *d_H = nullptr, *d_P = nullptr, *d_F = nullptr;
-  double *d_V = nullptr, *d_T = nullptr, *d_eig = nullptr;
+  double *d_V = nullptr, *d_T = nullptr, *d_eig = nullptr, *d_W = nullptr;
   double *d_eel = nullptr, *d_ecc = nullptr;
   int *d_niter = nullptr, *d_conv = nullptr, *d_status = nullptr;
   unsigned long long *d_tb = nullptr, *d_te = nullptr;
@@ -100,7 +103,7 @@ struct sgb_batch {
   bool profiling = false;
   double* d_hist = nullptr;
   int hist_stride = 0;
-  int64_t n_ints = 0, n_pk = 0, n_sq = 0, n_ao = 0;
+  int64_t n_ints = 0, n_pk = 0, n_sq = 0, n_ao = 0, n_w = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   float last_ms = 0.f;
 };
@@ -176,7 +179,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->nmol = nmol;
   b->desc.resize(nmol);
   b->natoms.assign(natoms, natoms + nmol);
-  int64_t atom0 = 0, blk0 = 0, pk0 = 0, sq0 = 0, ao0 = 0;
+  int64_t atom0 = 0, blk0 = 0, pk0 = 0, sq0 = 0, ao0 = 0, w0 = 0;
   std::vector<int8_t> slot;
   std::vector<int> first, hb;
   std::vector<int64_t> row_off;
@@ -217,6 +220,8 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     d.pk0 = pk0;
     d.sq0 = sq0;
     d.ao0 = ao0;
+    d.w0 = w0;
+    if (nao > kGsmemMax) w0 += ((int64_t)nao * nao + 31) / 32 * 32;
     blk0 += (roff + 31) / 32 * 32;
     pk0 += (tri(nao) + 31) / 32 * 32;
     sq0 += ((int64_t)nao * nao + 31) / 32 * 32;
@@ -225,7 +230,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     b->nmax = std::max(b->nmax, nao);
   }
   b->natoms_total = atom0;
-  b->n_ints = blk0; b->n_pk = pk0; b->n_sq = sq0; b->n_ao = ao0;
+  b->n_ints = blk0; b->n_pk = pk0; b->n_sq = sq0; b->n_ao = ao0; b->n_w = w0;
   b->hist_stride = hist_stride;
   // order: grouped by size class, largest estimated cost first within a class
   b->order.resize(nmol);
@@ -251,7 +256,8 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
                o_pos = take(24 * NA), o_first = take(4 * NA), o_roff = take(8 * NA),
                o_hb = take(4 * NA), o_ints = take(8 * b->n_ints), o_H = take(8 * b->n_pk),
                o_P = take(8 * b->n_pk), o_F = take(8 * b->n_pk), o_V = take(8 * b->n_sq),
-               o_T = take(8 * b->n_sq), o_eig = take(8 * b->n_ao), o_eel = take(8 * nmol),
+               o_T = take(8 * b->n_sq), o_W = take(8 * b->n_w), o_eig = take(8 * b->n_ao),
+               o_eel = take(8 * nmol),
                o_ecc = take(8 * nmol), o_nit = take(4 * nmol), o_conv = take(4 * nmol),
                o_stat = take(4 * nmol), o_tb = take(8 * nmol), o_te = take(8 * nmol),
                o_stage = take(8 * (size_t)kStageSlots * nmol),
@@ -291,6 +297,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->d_F = (double*)(base + o_F);
   b->d_V = (double*)(base + o_V);
   b->d_T = (double*)(base + o_T);
+  b->d_W = b->n_w ? (double*)(base + o_W) : nullptr;
   b->d_eig = (double*)(base + o_eig);
   b->d_eel = (double*)(base + o_eel);
   b->d_ecc = (double*)(base + o_ecc);
@@ -355,6 +362,7 @@ cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStre
 
 cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
                          cudaStream_t st) {
+  if (cr == 0) return launch_kernel<512, 0>(num_sms, a, smem, st);
   if (threads == 512) {
     switch (cr) {
       case 2: return launch_kernel<512, 2>(num_sms, a, smem, st);
@@ -376,9 +384,10 @@ cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, s
 int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_iter,
                   int sorted_vectors) {
   const bool scf = stages & STAGE_SCF;
-  if (scf && b->nmax > kSmallNmax)
+  if (scf && b->nmax > kBatchScfMax)
     return fail(ctx, SGB_E_UNSUPPORTED,
-                "SCF for nao=%d: the in-shared-memory path takes nao <= %d", b->nmax, kSmallNmax);
+                "SCF for nao=%d: one CTA per molecule takes nao <= %d (larger: sgb_scf's grid path)",
+                b->nmax, kBatchScfMax);
   BatchArgs a;
   a.mols = b->d_desc;
   a.slot = b->d_slot;
@@ -388,7 +397,7 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.hb = b->d_hb;
   a.ints = b->d_ints;
   a.H = b->d_H; a.P = b->d_P; a.F = b->d_F;
-  a.V = b->d_V; a.T = b->d_T; a.eig = b->d_eig;
+  a.V = b->d_V; a.T = b->d_T; a.eig = b->d_eig; a.W = b->d_W;
   a.e_el = b->d_eel; a.e_cc = b->d_ecc;
   a.n_iter = b->d_niter; a.converged = b->d_conv; a.status = b->d_status;
   a.hist = b->d_hist; a.hist_stride = b->hist_stride;
@@ -410,7 +419,9 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
     ac.nmol = cnt;
     ac.order = b->d_order + b->class_first[c];
     ac.counter = b->d_counter + c;
-    ac.nmax = std::max(1, b->class_nmax[c]);
+    // the Fock and SCF stages keep per-AO work vectors in shared memory; the others need
+    // only the reduction slots
+    ac.nmax = (stages & (STAGE_SCF | STAGE_FOCK)) ? std::max(1, b->class_nmax[c]) : 1;
     ac.mat_doubles = 0;
     if (scf)
       for (int q = 0; q < cnt; ++q)
@@ -1166,6 +1177,7 @@ int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int
   a.V = reinterpret_cast<double*>(base + o_V);
   a.T = reinterpret_cast<double*>(base + o_T);
   a.eig = reinterpret_cast<double*>(base + o_eig);
+  a.W = nullptr;
   a.e_el = &dr->e_el;
   a.e_cc = &dr->e_cc;
   a.n_iter = &dr->n_iter;

@@ -37,6 +37,7 @@ struct MolView {
   double* V;               // n*n, row-major: V[i*n + k] = AO i of vector k
   double* T;               // n*n scratch
   double* eig;             // n
+  double* W;               // n*n eigensolver work matrix in global memory (large molecules)
 };
 
 __device__ __forceinline__ int nao_of_slot(int s) { return s ? 4 : 1; }
@@ -465,11 +466,76 @@ __device__ __forceinline__ void rr_pair(int r, int k, int m, int& p, int& q) {
 // matrix only depends on the occupied subspace, which these rotations alone decide.
 // Each warp carries PP column pairs of a round at once (independent dependency chains
 // interleaved), which hides the latency of the dot-product reduction and the angle computation.
+// CR == 0: columns too long for registers (nao > 160, G and V in global memory); each pair is
+// streamed twice, once for the dot products and once for the rotation.
+template <int NT>
+__device__ void jacobi_pair_streamed(int n, double* gp, double* gq, double* vp, double* vq,
+                                     int lane, double rot_abs, double& worst) {
+  double app = 0.0, aqq = 0.0, apq = 0.0, aqp = 0.0;
+  for (int i = lane; i < n; i += 32) {
+    const double xg = gp[i], yg = gq[i], xv = vp[i], yv = vq[i];
+    app = fma(xv, xg, app);
+    aqq = fma(yv, yg, aqq);
+    apq = fma(xv, yg, apq);
+    aqp = fma(xg, yv, aqp);
+  }
+  warp_sum4(lane, app, aqq, apq, aqp);
+  const double a_pq = 0.5 * (apq + aqp);
+  if (!(fabs(a_pq) > rot_abs)) {
+    if (a_pq != a_pq) worst = INFINITY;
+    return;
+  }
+  worst = fmax(worst, fabs(a_pq));
+  const float num = (float)(2.0 * a_pq), den = (float)(aqq - app);
+  float tf = __fdividef(num, fabsf(den) + __fsqrt_rn(fmaf(den, den, num * num)));
+  if (den < 0.0f) tf = -tf;
+  const double t = (double)tf;
+  const double c = rsqrt(fma(t, t, 1.0)), sn = c * t;
+  for (int i = lane; i < n; i += 32) {
+    const double xg = gp[i], yg = gq[i], xv = vp[i], yv = vq[i];
+    gp[i] = c * xg - sn * yg;
+    gq[i] = sn * xg + c * yg;
+    vp[i] = c * xv - sn * yv;
+    vq[i] = sn * xv + c * yv;
+  }
+}
+
 template <int NT, int CR, int PP = 2>
 __device__ int block_jacobi_fv(int n, double* G, int ldg, double* V, int ldv, double* red,
                                double rot_abs, double done_abs, int max_sweeps,
                                const int* grp_a = nullptr, int na = 0, const int* grp_b = nullptr,
                                int nb = 0) {
+  if constexpr (CR == 0) {
+    const int ne = n + (n & 1), m = ne - 1, n2 = ne / 2;
+    const bool bip = grp_a != nullptr;
+    const int rounds = bip ? nb : m, per_round = bip ? na : n2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int sweep = 0; sweep < max_sweeps; ++sweep) {
+      double worst = 0.0;
+      for (int r = 0; r < rounds; ++r) {
+        for (int k = warp; k < per_round; k += NT / 32) {
+          int p, q;
+          if (bip) {
+            p = grp_a[k];
+            int j = k + r;
+            if (j >= nb) j -= nb;
+            q = grp_b[j];
+          } else {
+            rr_pair(r, k, m, p, q);
+            if (p >= n || q >= n) continue;
+          }
+          jacobi_pair_streamed<NT>(n, G + (int64_t)p * ldg, G + (int64_t)q * ldg,
+                                   V + (int64_t)p * ldv, V + (int64_t)q * ldv, lane, rot_abs,
+                                   worst);
+        }
+        __syncthreads();
+      }
+      worst = block_max<NT>(worst, red);
+      if (!(worst < INFINITY)) return -1;
+      if (worst < done_abs) return sweep + 1;
+    }
+    return -1;
+  } else {
   const int ne = n + (n & 1), m = ne - 1, n2 = ne / 2;
   const bool bip = grp_a != nullptr;
   const int rounds = bip ? nb : m, per_round = bip ? na : n2;
@@ -572,6 +638,7 @@ __device__ int block_jacobi_fv(int n, double* G, int ldg, double* V, int ldv, do
     if (worst < done_abs) return sweep + 1;
   }
   return -1;
+  }
 }
 
 // eig[i] = g_i . v_i - mu (one warp per column)

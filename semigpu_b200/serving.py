@@ -6,8 +6,9 @@ A free worker takes every request waiting in the queue -- up to `max_batch` mole
 its share of the HBM budget, by each molecule's device footprint -- builds one device batch
 (integrals, Hcore, P, F, eigenvectors stay resident for the whole SCF) and runs it; requests
 that arrive meanwhile wait for the next free worker, so batches form continuously from whatever
-has arrived (continuous batching at launch granularity).  Molecules above the in-CTA size limit
-run through the single-molecule grid path in the worker that picked them.
+has arrived (continuous batching at launch granularity).  Molecules up to nao 1024 share the
+batch (one CTA each); larger ones run through the single-molecule grid path in the worker that
+picked them.
 
 Latency of a request = completion time - arrival time (host clock); `stats()` reports p50/p99
 and throughput.  `replay()` drives an open-loop arrival schedule (e.g. Poisson) in real time.
@@ -24,17 +25,19 @@ import numpy as np
 from . import Context, Molecule, run_molecules
 from .geometry import Molecule as Geometry
 
-CTA_MAX_NAO = 160  # larger molecules take the grid path
+CTA_MAX_NAO = 1024  # larger molecules take the grid path
+SMEM_MAX_NAO = 160  # above this a batched molecule also holds an n x n eigensolver work matrix
 
 
 def device_bytes(mol: Geometry) -> int:
     """Device memory a molecule occupies inside a batch (integral blocks, Hcore/P/F packed,
-    eigenvectors + F full square, eigenvalues, atom arrays)."""
+    eigenvectors + F full square (+ the work matrix above nao 160), eigenvalues, atom arrays)."""
     heavy = int(np.count_nonzero(mol.Z > 1))
     light = mol.natoms - heavy
     nblk = 100 * heavy * (heavy + 1) // 2 + 10 * heavy * light + light * (light + 1) // 2
     n = mol.nao
-    return 8 * (nblk + 3 * n * (n + 1) // 2 + 2 * n * n + n) + 64 * mol.natoms + 256
+    squares = 3 if n > SMEM_MAX_NAO else 2
+    return 8 * (nblk + 3 * n * (n + 1) // 2 + squares * n * n + n) + 64 * mol.natoms + 256
 
 
 @dataclass
