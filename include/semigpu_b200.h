@@ -61,6 +61,17 @@ int sgb_ctx_destroy(sgb_ctx *ctx);
 int sgb_ctx_synchronize(sgb_ctx *ctx);
 const char *sgb_last_error(const sgb_ctx *ctx);
 const char *sgb_status_string(int status);
+/* How an SCF step gets the density P from F (no counterpart in the reference, which always
+ * diagonalises with LAPACK dsyev, scfcalculation.cpp:94-110):
+ *   SGB_SOLVER_PURIFY (default) -- trace-correcting purification on the FP64 tensor-core path
+ *     for nao <= 160 (the same aufbau projector; a Jacobi eigensolve replaces it for a step
+ *     where it does not converge, and gives the eigenpairs at the end of sgb_scf);
+ *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step.
+ * Molecules above nao 160 always diagonalise.  The environment variable
+ * SGB_DENSITY_SOLVER=jacobi changes the default (also for sgb_scf_noalloc). */
+#define SGB_SOLVER_PURIFY 0
+#define SGB_SOLVER_JACOBI 1
+int sgb_ctx_set_density_solver(sgb_ctx *ctx, int solver);
 /* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
  * it instead of allocating, and releasing the batch does not free device memory (cudaFree
  * synchronises the whole device, which would stall other contexts' work).  One batch at a time
@@ -168,10 +179,11 @@ int sgb_batch_last_ms(const sgb_batch *b, float *ms);
 int sgb_batch_timestamps(sgb_ctx *ctx, sgb_batch *b, unsigned long long *t_begin,
                          unsigned long long *t_end);
 /* Stage timers (the reference prints per-step Lapack/Pmat/Fmat/Ener times,
- * scfcalculation.cpp:83-140).  When on, each run records per molecule SGB_STAGE_SLOTS SM-cycle
- * counters: integrals, Hcore, Fock+energy, warm-start product, Jacobi, eigenvalues+sort,
- * density, core-core, then counts: Jacobi sweeps, occupied-virtual eigensolves, full ones. */
-#define SGB_STAGE_SLOTS 11
+ * scfcalculation.cpp:83-140).  When on, each run records per molecule SGB_STAGE_SLOTS
+ * counters: SM cycles of integrals, Hcore, Fock+energy, warm-start product, Jacobi,
+ * eigenvalues+sort, density, core-core, purification; then counts: Jacobi sweeps,
+ * occupied-virtual eigensolves, full eigensolves, purification products. */
+#define SGB_STAGE_SLOTS 13
 int sgb_batch_set_profiling(sgb_batch *b, int on);
 int sgb_batch_stage_cycles(sgb_ctx *ctx, sgb_batch *b, unsigned long long *cycles);
 /* Device pointer of the batch's coordinate buffer (natoms_total*3 doubles) for callers that

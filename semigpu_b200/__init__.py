@@ -25,6 +25,7 @@ OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN = (
     0, -1, -2, -3, -4, -5, -6, 1, 2)
 BLOCKS, HCORE, FOCK, DENSITY, EIGVAL, EIGVEC = range(6)
 PATH_AUTO, PATH_CTA, PATH_GRID = range(3)
+SOLVER_PURIFY, SOLVER_JACOBI = range(2)
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -39,6 +40,7 @@ SIGNATURES = {
     "sgb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
     "sgb_ctx_reserve": (ctypes.c_int, [_VP, ctypes.c_size_t]),
+    "sgb_ctx_set_density_solver": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_heat_of_formation": (ctypes.c_int, [ctypes.c_int, _I, ctypes.c_double, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
@@ -142,6 +144,10 @@ class Context:
 
     def synchronize(self):
         self.check(lib().sgb_ctx_synchronize(self.h), "synchronize")
+
+    def set_density_solver(self, solver: int):
+        """SOLVER_PURIFY (default) or SOLVER_JACOBI for the SCF steps of later calls."""
+        self.check(lib().sgb_ctx_set_density_solver(self.h, int(solver)), "set_density_solver")
 
     def reserve(self, nbytes: int):
         """Reusable device arena for batches of up to `nbytes` (see sgb_ctx_reserve)."""
@@ -305,14 +311,17 @@ class Batch:
         return tb, te
 
     STAGES = ("integrals", "hcore", "fock", "warm_gemm", "jacobi", "eigval_sort", "density",
-              "core_core", "sweeps", "bipartite_solves", "full_solves")
+              "core_core", "purify", "sweeps", "bipartite_solves", "full_solves",
+              "purify_products")
+    TIMED_STAGES = 9  # the first nine are SM cycles, the rest counts
 
     def set_profiling(self, on: bool = True):
         lib().sgb_batch_set_profiling(self.h, int(on))
 
     def stage_cycles(self) -> np.ndarray:
-        """(nmol, 11) per-stage SM cycles of the last run, then counts (Jacobi sweeps,
-        occupied-virtual eigensolves, full eigensolves)."""
+        """(nmol, 13): per-stage SM cycles of the last run (the first TIMED_STAGES columns),
+        then counts (Jacobi sweeps, occupied-virtual eigensolves, full eigensolves,
+        purification products)."""
         out = np.zeros((self.nmol, len(self.STAGES)), np.uint64)
         self.ctx.check(lib().sgb_batch_stage_cycles(
             self.ctx.h, self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_ulonglong))),

@@ -10,10 +10,16 @@
 //
 // The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
 // repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
-// max_iter steps.  The eigensolve is a cyclic Jacobi on V^T F V carried on the columns of V and
-// G = F V; after the first step it is warm-started from the previous eigenvectors, which the
-// new F barely mixes, so it needs few sweeps.
+// max_iter steps.  Two ways to get P from F, chosen per launch:
+//  * SOLVER_PURIFY (default, nao <= 160): P by trace-correcting purification, ~20 symmetric
+//    matrix squares on the FP64 tensor-core path (purify.cuh); a Jacobi eigensolve replaces it
+//    for a step whose purification fails (vanishing gap), and runs once at the end when the
+//    eigenpairs are wanted (single-molecule calls).
+//  * SOLVER_JACOBI: a cyclic Jacobi on V^T F V carried on the columns of V and G = F V; after
+//    the first step it is warm-started from the previous eigenvectors, which the new F barely
+//    mixes, so it needs few sweeps.  Molecules above nao 160 always take this one.
 #pragma once
+#include "purify.cuh"
 #include "scf_block.cuh"
 
 namespace sgb {
@@ -47,7 +53,8 @@ struct BatchArgs {
   int max_iter;
   int nmax;         // largest nao in the launch (sizes the shared memory)
   size_t mat_doubles;  // shared matrix region (max over molecules of mat_doubles_for)
-  int sorted_vectors;
+  int sorted_vectors;  // eigenvalues and sorted eigenvectors of the last eigensolve wanted
+  int solver;       // SOLVER_*
   int stages;       // STAGE_* bits
   unsigned long long* t_begin;  // optional per-molecule %globaltimer (ns) at start / end
   unsigned long long* t_end;
@@ -58,7 +65,9 @@ struct BatchArgs {
 // analogue of the reference's per-step Lapack/Pmat/Fmat/Ener timers
 // (scfcalculation.cpp:83-140).
 enum : int { ST_INTS = 0, ST_HCORE, ST_FOCK, ST_SHIFT_GEMM, ST_JACOBI, ST_EIGVAL_SORT,
-             ST_DENSITY, ST_CORECORE, ST_SWEEPS, ST_BIPARTITE, ST_FULLJAC, kStageSlots };
+             ST_DENSITY, ST_CORECORE, ST_PURIFY, ST_SWEEPS, ST_BIPARTITE, ST_FULLJAC,
+             ST_PURIFY_PRODUCTS, kStageSlots };
+constexpr int kTimedSlots = ST_PURIFY + 1;  // slots [0, kTimedSlots) are cycles, the rest counts
 
 struct StageClock {
   unsigned long long* out;
@@ -86,6 +95,8 @@ enum : int { STAGE_INTS = 1, STAGE_HCORE = 2, STAGE_SCF = 4, STAGE_CC = 8, STAGE
              STAGE_FOCK = 16 /* F and E_el from the P already in device memory */ };
 
 enum : int { MOL_OK = 0, MOL_EIG_FAILED = 1, MOL_NAN = 2 };
+
+enum : int { SOLVER_PURIFY = 0, SOLVER_JACOBI = 1 };
 
 __host__ __device__ inline int smem_ld(int n) { return n | 1; }
 
@@ -118,7 +129,9 @@ constexpr int kGsmemMax = 160;
 __host__ __device__ inline size_t mat_doubles_for(int n) {
   const size_t ld = (size_t)smem_ld(n);
   if (n > kGsmemMax) return 0;
-  return (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
+  const size_t jac = (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
+  const size_t pur = purify_doubles(n);  // the purification's X shares the region
+  return jac > pur ? jac : pur;
 }
 
 __host__ __device__ inline size_t extra_doubles(int nmax) {
@@ -247,68 +260,91 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     E = block_fock_energy<NT>(m, Ffull, n, wq, red);
     clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
+    // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
+    const bool purify = PLACE != 2 && a.solver == SOLVER_PURIFY;
     while (!conv && steps < a.max_iter) {
-      // ---- eigensolve of F: Jacobi on V^T F V through (V, G = F V), V warm-started ----
-      if (steps == 0) {
-        for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-          const int j = t / n, i = t % n;
-          V[(int64_t)j * ldv + i] = i == j ? 1.0 : 0.0;
-          G[(int64_t)j * ld + i] = Ffull[t];
-        }
-      } else {
-        block_shifted_product(n, Ffull, 0.0, V, ldv, G, ld);
-      }
-      __syncthreads();
-      clk.lap(ST_SHIFT_GEMM);
-      const int nocc = m.nocc, nvir = n - nocc;
-      int sw;
-      bool full = steps < kFullJacobiSteps || a.sorted_vectors || nocc == 0 || nvir == 0;
-      if (!full) {
-        // occupied / virtual split of the warm-started columns by their Rayleigh quotients
-        block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
-        __syncthreads();
-        split_by_rank(dval, n, nocc, occ, vir);
-        __syncthreads();
-        const bool o_small = nocc <= nvir;
-        sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneGapped, 40,
-                                     o_small ? occ : vir, o_small ? nocc : nvir,
-                                     o_small ? vir : occ, o_small ? nvir : nocc);
-        if (sw >= 0) {
-          clk.add(ST_BIPARTITE, 1);
-          // the occupied block must still hold the lowest states (no level crossing)
-          block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+      bool cold = steps == 0, jacobi = !purify;
+      if (purify) {
+        // ---- P from F by purification; a Jacobi eigensolve if that fails ----
+        const int prod = block_purify<NT>(Ffull, n, m.nocc, smem, red);
+        clk.lap(ST_PURIFY);
+        clk.add(ST_PURIFY_PRODUCTS, (unsigned long long)(prod > 0 ? prod : 0));
+        if (prod >= 0) {
+          purify_density(smem, n, m.P);
           __syncthreads();
-          double hi = -INFINITY, lo = INFINITY;
-          for (int i = threadIdx.x; i < nocc; i += blockDim.x) hi = fmax(hi, dval[occ[i]]);
-          for (int i = threadIdx.x; i < nvir; i += blockDim.x) lo = fmin(lo, dval[vir[i]]);
-          hi = block_max<NT>(hi, red);
-          lo = -block_max<NT>(-lo, red);
-          full = !(hi + kCrossMargin < lo);
+          clk.lap(ST_DENSITY);
+        } else {
+          jacobi = cold = true;
         }
       }
-      if (full) {
-        clk.add(ST_FULLJAC, 1);
-        sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
-        if (sw >= 0) {
+      if (jacobi) {
+        // ---- eigensolve of F: Jacobi on V^T F V through (V, G = F V), V warm-started ----
+        if (cold) {
+          for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+            const int j = t / n, i = t % n;
+            V[(int64_t)j * ldv + i] = i == j ? 1.0 : 0.0;
+            G[(int64_t)j * ld + i] = Ffull[t];
+          }
+        } else {
+          block_shifted_product(n, Ffull, 0.0, V, ldv, G, ld);
+        }
+        __syncthreads();
+        clk.lap(ST_SHIFT_GEMM);
+        const int nocc = m.nocc, nvir = n - nocc;
+        int sw;
+        bool full = cold || steps < kFullJacobiSteps || a.sorted_vectors || nocc == 0 || nvir == 0;
+        if (!full) {
+          // occupied / virtual split of the warm-started columns by their Rayleigh quotients
           block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
           __syncthreads();
           split_by_rank(dval, n, nocc, occ, vir);
+          __syncthreads();
+          const bool o_small = nocc <= nvir;
+          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneGapped, 40,
+                                       o_small ? occ : vir, o_small ? nocc : nvir,
+                                       o_small ? vir : occ, o_small ? nvir : nocc);
+          if (sw >= 0) {
+            clk.add(ST_BIPARTITE, 1);
+            // the occupied block must still hold the lowest states (no level crossing)
+            block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+            __syncthreads();
+            double hi = -INFINITY, lo = INFINITY;
+            for (int i = threadIdx.x; i < nocc; i += blockDim.x) hi = fmax(hi, dval[occ[i]]);
+            for (int i = threadIdx.x; i < nvir; i += blockDim.x) lo = fmin(lo, dval[vir[i]]);
+            hi = block_max<NT>(hi, red);
+            lo = -block_max<NT>(-lo, red);
+            full = !(hi + kCrossMargin < lo);
+          }
         }
+        if (full) {
+          clk.add(ST_FULLJAC, 1);
+          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
+          if (sw >= 0) {
+            block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+            __syncthreads();
+            split_by_rank(dval, n, nocc, occ, vir);
+          }
+        }
+        clk.lap(ST_JACOBI);
+        clk.add(ST_SWEEPS, (unsigned long long)(sw > 0 ? sw : 0));
+        if (sw < 0) { status = MOL_EIG_FAILED; break; }
+        __syncthreads();
+        clk.lap(ST_EIGVAL_SORT);
+        // ---- density from the occupied vectors, gathered into the G region ----
+        for (int t = threadIdx.x; t < n * m.nocc; t += blockDim.x) {
+          const int k = t / n, i = t % n;
+          G[(int64_t)k * ld + i] = V[(int64_t)occ[k] * ldv + i];
+        }
+        __syncthreads();
+        block_density(n, m.nocc, G, ld, m.P);
+        __syncthreads();
+        clk.lap(ST_DENSITY);
       }
-      clk.lap(ST_JACOBI);
-      clk.add(ST_SWEEPS, (unsigned long long)(sw > 0 ? sw : 0));
-      if (sw < 0) { status = MOL_EIG_FAILED; break; }
-      __syncthreads();
-      clk.lap(ST_EIGVAL_SORT);
-      // ---- density from the occupied vectors, gathered into the G region ----
-      for (int t = threadIdx.x; t < n * m.nocc; t += blockDim.x) {
-        const int k = t / n, i = t % n;
-        G[(int64_t)k * ld + i] = V[(int64_t)occ[k] * ldv + i];
+      // the F just diagonalised, kept for the eigenpairs reported at the end
+      if (purify && a.sorted_vectors) {
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x) m.V[t] = Ffull[t];
+        __syncthreads();
       }
-      __syncthreads();
-      block_density(n, m.nocc, G, ld, m.P);
-      __syncthreads();
-      clk.lap(ST_DENSITY);
       // ---- Fock + energy ----
       const double Eold = E;
       E = block_fock_energy<NT>(m, Ffull, n, wq, red);
@@ -318,9 +354,31 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       if (E != E) { status = MOL_NAN; break; }
       conv = fabs(Eold - E) < a.tol;
     }
+    if (purify && a.sorted_vectors && steps > 0 && status == MOL_OK) {
+      // eigenpairs of the last F that produced a density (saved in m.V): one full Jacobi
+      for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int j = t / n, i = t % n;
+        G[(int64_t)j * ld + i] = m.V[t];
+      }
+      __syncthreads();
+      for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int j = t / n, i = t % n;
+        V[(int64_t)j * ldv + i] = i == j ? 1.0 : 0.0;
+      }
+      __syncthreads();
+      clk.start();
+      clk.add(ST_FULLJAC, 1);
+      const int sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
+      clk.add(ST_SWEEPS, (unsigned long long)(sw > 0 ? sw : 0));
+      if (sw < 0) status = MOL_EIG_FAILED;
+      else block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
+      __syncthreads();
+      clk.lap(ST_JACOBI);
+    }
     // eigenvalues (ascending) and, on request, the eigenvectors sorted the same way into T
-    // (column k = vector k, the layout of SCFCalculation::eigenVec)
-    if (steps > 0) {
+    // (column k = vector k, the layout of SCFCalculation::eigenVec); with purification only
+    // when requested (dval is not computed otherwise)
+    if (steps > 0 && (!purify || a.sorted_vectors) && status == MOL_OK) {
       __syncthreads();
       for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const int rank = ascending_rank(dval, n, i);

@@ -37,6 +37,12 @@ constexpr SizeClass kClasses[] = {{64, 2, 512},   {96, 3, 512},        {128, 4, 
 constexpr int kNumClasses = 6;
 constexpr int kBatchScfMax = 1024;  // one CTA per molecule up to here; the grid path above
 
+// SGB_SOLVER_PURIFY unless the environment sets SGB_DENSITY_SOLVER=jacobi.
+int default_solver() {
+  const char* env = getenv("SGB_DENSITY_SOLVER");
+  return env && strcmp(env, "jacobi") == 0 ? SOLVER_JACOBI : SOLVER_PURIFY;
+}
+
 int class_of(int nao) {
   int c = 0;
   while (nao > kClasses[c].nmax) ++c;
@@ -65,6 +71,7 @@ struct sgb_ctx {
   cudaStream_t aux[kNumClasses] = {};
   cudaEvent_t joined[kNumClasses] = {};
   int class_threads[kNumClasses] = {};
+  int solver = SOLVER_PURIFY;  // SGB_SOLVER_*
   // optional reusable arena (sgb_ctx_reserve): a batch that fits takes it instead of calling
   // cudaMalloc, and gives it back without cudaFree (which would synchronise the device)
   char* pool = nullptr;
@@ -404,6 +411,7 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.tol = tol;
   a.max_iter = std::min(max_iter, b->hist_stride > 0 ? b->hist_stride - 1 : max_iter);
   a.sorted_vectors = sorted_vectors;
+  a.solver = ctx->solver;
   a.stages = stages;
   a.t_begin = b->d_tb;
   a.t_end = b->d_te;
@@ -752,6 +760,7 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
       return SGB_E_CUDA;
     }
   }
+  c->solver = default_solver();
   if (const char* env = getenv("SGB_CLASS_THREADS")) {  // e.g. "256,512,512,512"
     int k = 0;
     for (const char* p = env; *p && k < kNumClasses; ++k) {
@@ -762,6 +771,14 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
     }
   }
   *out = c;
+  return SGB_OK;
+}
+
+int sgb_ctx_set_density_solver(sgb_ctx* ctx, int solver) {
+  if (!ctx) return SGB_E_ARG;
+  if (solver != SGB_SOLVER_PURIFY && solver != SGB_SOLVER_JACOBI)
+    return fail(ctx, SGB_E_ARG, "unknown density solver %d", solver);
+  ctx->solver = solver == SGB_SOLVER_JACOBI ? SOLVER_JACOBI : SOLVER_PURIFY;
   return SGB_OK;
 }
 
@@ -1190,6 +1207,7 @@ int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int
   a.nmax = nao;
   a.mat_doubles = mat_doubles_for(nao);
   a.sorted_vectors = 0;
+  a.solver = default_solver();
   a.stages = STAGE_ALL;
   a.t_begin = nullptr;
   a.t_end = nullptr;

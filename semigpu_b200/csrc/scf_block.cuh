@@ -78,7 +78,7 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 
 // ------------------------------------------------------------------------------------------
 // Integrals: one thread per atom pair (A >= B), writing the pair's block.
-__device__ inline void write_pair_block(const MolView& m, int A, int B) {
+__device__ __noinline__ void write_pair_block(const MolView& m, int A, int B) {
   double* blk = m.ints + block_offset(m.row_off, m.hb, m.slot, A, B);
   const int sA = m.slot[A], sB = m.slot[B];
   if (A == B) {
@@ -131,7 +131,7 @@ __device__ __forceinline__ double coulomb_ss(const MolView& m, int A, int pq, in
 
 // Hcore: off-diagonal atom blocks 1/2 (beta_mu + beta_nu) S_mu_nu (hcore.cpp:38-69), diagonal
 // atom blocks U delta + sum_{C != A} -Z_C (mu nu|s_C s_C) (hcore.cpp:71-92).
-__device__ inline void hcore_offdiag_pair(const MolView& m, int A, int B) {
+__device__ __noinline__ void hcore_offdiag_pair(const MolView& m, int A, int B) {
   const int sA = m.slot[A], sB = m.slot[B];
   double S[16];
   overlap_block(sA, sB, m.pos + 3 * A, m.pos + 3 * B, S);
@@ -145,7 +145,7 @@ __device__ inline void hcore_offdiag_pair(const MolView& m, int A, int B) {
   }
 }
 
-__device__ inline void hcore_diag_atom(const MolView& m, int A, int pq) {
+__device__ __noinline__ void hcore_diag_atom(const MolView& m, int A, int pq) {
   const int sA = m.slot[A];
   double s = 0.0;
   for (int C = 0; C < m.natoms; ++C)
@@ -192,7 +192,7 @@ __device__ __forceinline__ void pair_density_task(const MolView& m, double* wq, 
 
 // Diagonal atom block element (A, pq): Coulomb over every atom plus one-center exchange.
 // Returns the element's share of E_el.
-__device__ inline double fock_diag_task(const MolView& m, const double* wq, double* Fs,
+__device__ __noinline__ double fock_diag_task(const MolView& m, const double* wq, double* Fs,
                                         int64_t ld, int t) {
   const int A = t / 10, pq = t % 10;
   const int sA = m.slot[A];
@@ -239,7 +239,7 @@ __device__ inline double fock_diag_task(const MolView& m, const double* wq, doub
 }
 
 // Off-diagonal atom block (A > B): two-center exchange only.  Returns its share of E_el.
-__device__ inline double fock_pair_task(const MolView& m, double* Fs, int64_t ld, int A, int B) {
+__device__ __noinline__ double fock_pair_task(const MolView& m, double* Fs, int64_t ld, int A, int B) {
   const int sA = m.slot[A], sB = m.slot[B], fA = m.first[A], fB = m.first[B];
   const double* I = blk_ptr(m, A, B);
   const int nA = nao_of_slot(sA), nB = nao_of_slot(sB);
@@ -302,7 +302,7 @@ __device__ inline void block_guess(const MolView& m) {
 
 // Core-core repulsion of atoms Al < Bh (corecorerepulsion.cpp:12-65):
 // Z_A Z_B (s_A s_A|s_B s_B) f(R), R in Angstrom; N-H / O-H use 1 + R exp(-alpha_X R) + exp(-alpha_H R).
-__device__ inline double core_core_pair(const MolView& m, int Bh, int Al) {
+__device__ __noinline__ double core_core_pair(const MolView& m, int Bh, int Al) {
   const int sa = m.slot[Al], sb = m.slot[Bh];
   const double gam = *blk_ptr(m, Bh, Al);
   const double* pa = m.pos + 3 * Al;
