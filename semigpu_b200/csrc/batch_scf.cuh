@@ -137,7 +137,7 @@ __host__ __device__ inline size_t mat_doubles_for(int n) {
 __host__ __device__ inline size_t extra_doubles(int nmax) {
   return 3 * (size_t)nmax + 8   // wq (<= 2.5 n) + pad
          + (size_t)nmax          // eigenvalues of the last eigensolve
-         + 32                    // reductions
+         + 64                    // reductions (two halves of 32)
          + (size_t)nmax + 2;     // occupied and virtual index lists (ints, two per double)
 }
 
@@ -233,7 +233,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   double* wq = smem + a.mat_doubles;
   double* dval = wq + 3 * nmax + 8;
   double* red = dval + nmax;
-  int* occ = reinterpret_cast<int*>(red + 32);
+  int* occ = reinterpret_cast<int*>(red + 64);
   int* vir = occ + nmax + 2;
   double* Ffull = m.T;  // F as a full n x n matrix, global scratch
   if (a.t_begin && threadIdx.x == 0) a.t_begin[mi] = global_ns();
@@ -413,7 +413,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
 
 // NT threads per CTA; CR column registers per lane in the eigensolver (nao <= 32 * CR).
 template <int NT, int CR>
-__global__ void __launch_bounds__(NT, 1) k_batch_scf(BatchArgs a) {
+__global__ void __launch_bounds__(NT, 512 / NT) k_batch_scf(BatchArgs a) {
   extern __shared__ double smem[];
   __shared__ int s_next;
   for (;;) {

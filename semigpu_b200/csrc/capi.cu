@@ -25,16 +25,17 @@ namespace {
 constexpr int kSmallNmax = 160;  // largest nao whose n x n FP64 matrix fits one CTA's smem
 
 // Size classes of the batched launch, by nao: (upper bound, eigenvector column registers per
-// lane, default threads per CTA).  Up to nao 160 the eigensolver's columns sit in registers
-// and shared memory; the class up to 1024 streams them from global memory (CR 0).  The last
-// class holds molecules too large for one CTA's SCF; only the integral, Hcore, Fock and
-// core-core stages run there (their SCF is the grid path of sgb_scf).
+// lane, default threads per CTA; smaller molecules take smaller CTAs, several per SM).  Up to
+// nao 160 the eigensolver's columns sit in registers and shared memory; the class up to 1024
+// streams them from global memory (CR 0).  The last class holds molecules too large for one
+// CTA's SCF; only the integral, Hcore, Fock and core-core stages run there (their SCF is the
+// grid path of sgb_scf).
 struct SizeClass {
   int nmax, cr, threads;
 };
-constexpr SizeClass kClasses[] = {{64, 2, 512},   {96, 3, 512},        {128, 4, 512}, {160, 5, 512},
-                                  {1024, 0, 512}, {1 << 30, 0, 512}};
-constexpr int kNumClasses = 6;
+constexpr SizeClass kClasses[] = {{32, 2, 128},  {64, 2, 256},   {96, 3, 512},     {128, 4, 512},
+                                  {160, 5, 512}, {1024, 0, 512}, {1 << 30, 0, 512}};
+constexpr int kNumClasses = 7;
 constexpr int kBatchScfMax = 1024;  // one CTA per molecule up to here; the grid path above
 
 // SGB_SOLVER_PURIFY unless the environment sets SGB_DENSITY_SOLVER=jacobi.
@@ -370,6 +371,7 @@ cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStre
 cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
                          cudaStream_t st) {
   if (cr == 0) return launch_kernel<512, 0>(num_sms, a, smem, st);
+  if (threads == 128 && cr == 2) return launch_kernel<128, 2>(num_sms, a, smem, st);
   if (threads == 512) {
     switch (cr) {
       case 2: return launch_kernel<512, 2>(num_sms, a, smem, st);
@@ -765,7 +767,7 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
     int k = 0;
     for (const char* p = env; *p && k < kNumClasses; ++k) {
       const int t = atoi(p);
-      if (t == 256 || t == 512) c->class_threads[k] = t;
+      if (t == 256 || t == 512 || (t == 128 && kClasses[k].cr == 2)) c->class_threads[k] = t;
       while (*p && *p != ',') ++p;
       if (*p == ',') ++p;
     }

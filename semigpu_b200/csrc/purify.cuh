@@ -104,10 +104,13 @@ __device__ void purify_init(const double* F, int n, double* X, int ld, double* r
 
 // X <- X^2 (sq) or 2X - X^2 (!sq), in place; t1, t2 <- trace and squared norm of the result.
 // MAXST: super-tiles per warp (the launch's count rounded up), so the accumulators of smaller
-// orders take fewer registers.
+// orders take fewer registers.  Two barriers per step: after the product (every warp has read
+// X) and after the write-back (X and the per-warp partial sums complete).  The partial sums
+// alternate between two halves of red (buf), so the next step's writes never meet this step's
+// reads.
 template <int NT, int MAXST>
 __device__ __noinline__ void purify_step(double* X, int n16, int ld, bool sq, double* red,
-                                         double& t1, double& t2) {
+                                         int buf, double& t1, double& t2) {
   constexpr int NW = NT / 32;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane >> 2, q = lane & 3;
@@ -161,13 +164,25 @@ __device__ __noinline__ void purify_step(double* X, int n16, int ld, bool sq, do
       }
     }
   }
-  block_sum2<NT>(s1, s2, red);  // its barriers also order the writes before the next read
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  double* part = red + 32 * buf;
+  if (lane == 0) { part[warp] = s1; part[16 + warp] = s2; }
+  __syncthreads();
+  s1 = 0.0;
+  s2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) { s1 += part[k]; s2 += part[16 + k]; }
   t1 = s1;
   t2 = s2;
 }
 
 // Purifies F (row-major n x n in global memory) into X = P / 2 in shared memory.  Returns the
-// number of products, or -1 (no convergence, wrong trace or a non-finite value).
+// number of products, or -1 (no convergence, wrong trace or a non-finite value).  red: 64
+// doubles.
 template <int NT>
 __device__ int block_purify(const double* F, int n, int nocc, double* X, double* red) {
   const int ld = purify_ld(n), n16 = purify_n16(n);
@@ -185,14 +200,17 @@ __device__ int block_purify(const double* F, int n, int nocc, double* X, double*
     constexpr int NW = NT / 32;
     constexpr int kSuper = (kPurifyMaxN16 / 16) * (kPurifyMaxN16 / 16 + 1) / 2;
     const int cnt = (n16 >> 4) * ((n16 >> 4) + 1) / 2;
+    const int buf = it & 1;
     if (cnt <= NW)
-      purify_step<NT, 1>(X, n16, ld, sq, red, t1, t2);
+      purify_step<NT, 1>(X, n16, ld, sq, red, buf, t1, t2);
     else if (cnt <= 2 * NW)
-      purify_step<NT, 2>(X, n16, ld, sq, red, t1, t2);
+      purify_step<NT, 2>(X, n16, ld, sq, red, buf, t1, t2);
     else if (cnt <= 3 * NW || (kSuper + NW - 1) / NW <= 3)
-      purify_step<NT, 3>(X, n16, ld, sq, red, t1, t2);
+      purify_step<NT, 3>(X, n16, ld, sq, red, buf, t1, t2);
+    else if constexpr (NT >= 256)
+      purify_step<NT, (kSuper + NW - 1) / NW>(X, n16, ld, sq, red, buf, t1, t2);
     else
-      purify_step<NT, (kSuper + NW - 1) / NW>(X, n16, ld, sq, red, t1, t2);
+      return -1;  // 128-thread CTAs only take nao <= 64 (at most 10 super-tiles)
   }
   return -1;
 }
