@@ -19,6 +19,7 @@
 //    the first step it is warm-started from the previous eigenvectors, which the new F barely
 //    mixes, so it needs few sweeps.  Molecules above nao 160 always take this one.
 #pragma once
+#include "fock_block.cuh"
 #include "purify.cuh"
 #include "scf_block.cuh"
 
@@ -126,19 +127,34 @@ constexpr double kJacobiDoneGapped = 3e-6;
 // Largest nao whose G fits one CTA's shared memory; above it G and V are global (streamed).
 constexpr int kGsmemMax = 160;
 
+// The Fock build keeps its staging buffers and heavy-heavy partial sums in the matrix region
+// while G (and X) are dead: from its start, or after G and V when G's part is too small (V,
+// in shared memory up to nao 110, must survive).  Above nao 160 the partial sums go to the
+// global work matrix instead.
+__host__ __device__ inline size_t fock_smem_doubles(int n) {
+  return (size_t)kFockStage + (n > kGsmemMax ? 0 : fock_xx_doubles(n));
+}
+__host__ __device__ inline size_t fock_stage_at(int n) {
+  const size_t g = (size_t)n * smem_ld(n);
+  return (n > kGsmemMax || n > kVsmemMax || g >= fock_smem_doubles(n)) ? 0 : 2 * g;
+}
+
 __host__ __device__ inline size_t mat_doubles_for(int n) {
   const size_t ld = (size_t)smem_ld(n);
-  if (n > kGsmemMax) return 0;
+  if (n > kGsmemMax) return kFockStage;
   const size_t jac = (n <= kVsmemMax ? 2 : 1) * (size_t)n * ld;
   const size_t pur = purify_doubles(n);  // the purification's X shares the region
-  return jac > pur ? jac : pur;
+  const size_t fk = fock_stage_at(n) + fock_smem_doubles(n);
+  const size_t m = jac > pur ? jac : pur;
+  return m > fk ? m : fk;
 }
 
 __host__ __device__ inline size_t extra_doubles(int nmax) {
-  return 3 * (size_t)nmax + 8   // wq (<= 2.5 n) + pad
+  return 2 * (3 * (size_t)nmax + 8)  // wq and J (each <= 2.5 n) + pad
          + (size_t)nmax          // eigenvalues of the last eigensolve
          + 64                    // reductions (two halves of 32)
-         + (size_t)nmax + 2;     // occupied and virtual index lists (ints, two per double)
+         + (size_t)nmax + 2      // occupied and virtual index lists (ints, two per double)
+         + (size_t)nmax / 8 + 2; // heavy atom list of the Fock build (ints)
 }
 
 __device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& d) {
@@ -231,10 +247,14 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   double* V = PLACE == 0 ? smem + (size_t)n * ld : m.V;
   const int ldv = PLACE == 0 ? ld : n;
   double* wq = smem + a.mat_doubles;
-  double* dval = wq + 3 * nmax + 8;
+  double* Jc = wq + 3 * nmax + 8;  // Coulomb sums of the Fock build
+  double* dval = Jc + 3 * nmax + 8;
+  double* stage = smem + fock_stage_at(n);
+  double* xs = PLACE == 2 ? m.W : stage + kFockStage;
   double* red = dval + nmax;
   int* occ = reinterpret_cast<int*>(red + 64);
   int* vir = occ + nmax + 2;
+  int* hv = vir + nmax + 2;
   double* Ffull = m.T;  // F as a full n x n matrix, global scratch
   if (a.t_begin && threadIdx.x == 0) a.t_begin[mi] = global_ns();
   StageClock clk{a.stage_cycles ? a.stage_cycles + (int64_t)mi * kStageSlots : nullptr, 0};
@@ -257,7 +277,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   if (a.stages & STAGE_SCF) {
     block_guess(m);
     __syncthreads();
-    E = block_fock_energy<NT>(m, Ffull, n, wq, red);
+    E = block_fock_energy<NT>(m, Ffull, n, wq, Jc, stage, xs, hv, red);
     clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
@@ -347,7 +367,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       }
       // ---- Fock + energy ----
       const double Eold = E;
-      E = block_fock_energy<NT>(m, Ffull, n, wq, red);
+      E = block_fock_energy<NT>(m, Ffull, n, wq, Jc, stage, xs, hv, red);
       clk.lap(ST_FOCK);
       ++steps;
       if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride + steps] = E;
@@ -389,7 +409,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     }
   }
   if (a.stages & STAGE_FOCK) {
-    E = block_fock_energy<NT>(m, nullptr, 0, wq, red);
+    E = block_fock_energy<NT>(m, nullptr, 0, wq, Jc, stage, xs, hv, red);
     if (threadIdx.x == 0) a.e_el[mi] = E;
   }
   double ecc = 0.0;

@@ -433,7 +433,7 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
     // only the reduction slots
     ac.nmax = (stages & (STAGE_SCF | STAGE_FOCK)) ? std::max(1, b->class_nmax[c]) : 1;
     ac.mat_doubles = 0;
-    if (scf)
+    if (stages & (STAGE_SCF | STAGE_FOCK))
       for (int q = 0; q < cnt; ++q)
         ac.mat_doubles = std::max(ac.mat_doubles,
                                   mat_doubles_for(b->desc[b->order[b->class_first[c] + q]].nao));

@@ -172,13 +172,13 @@ __device__ inline void block_hcore(const MolView& m) {
 
 // ------------------------------------------------------------------------------------------
 // Fock build + electronic energy.  Writes F packed to global memory and, when Fs != nullptr,
-// the full symmetric F (leading dimension ld); the CTA version returns E_el in every thread.
+// the full symmetric F (leading dimension ld).
 //
 // wq: scratch of 10 * nheavy + nlight doubles: the pair densities of each atom,
 //     w_C[q] = P_{lam sig} (x2 when lam != sig) for pair q = (lam, sig) of atom C.
 __device__ __forceinline__ int wq_offset(const MolView& m, int A) { return 9 * m.hb[A] + A; }
 
-// Per-task pieces (used by the CTA path below and by the grid-wide kernels).
+// Per-task pieces of the grid-wide kernels (the one-CTA build is in fock_block.cuh).
 
 // w_C[q] for task t = (C, q)
 __device__ __forceinline__ void pair_density_task(const MolView& m, double* wq, int t) {
@@ -271,22 +271,6 @@ __device__ __noinline__ double fock_pair_task(const MolView& m, double* Fs, int6
       e += m.P[ij] * (h + fv);
     }
   return e;
-}
-
-template <int NT>
-__device__ double block_fock_energy(const MolView& m, double* Fs, int ld, double* wq,
-                                    double* red) {
-  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) pair_density_task(m, wq, t);
-  __syncthreads();
-  double e = 0.0;
-  for (int t = threadIdx.x; t < m.natoms * 10; t += blockDim.x) e += fock_diag_task(m, wq, Fs, ld, t);
-  const int64_t np = tri(m.natoms);
-  for (int64_t p = threadIdx.x; p < np; p += blockDim.x) {
-    int A, B;
-    tri_inverse(p, A, B);
-    if (A != B) e += fock_pair_task(m, Fs, ld, A, B);
-  }
-  return block_sum<NT>(e, red);
 }
 
 // Initial guess P_ii = Z_A / nAO_A, zero elsewhere (densitymatrix.cpp:26-37).
