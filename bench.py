@@ -341,11 +341,16 @@ def run_ours(args):
         # plain FP64 GPU path: one molecule at a time through the stage API (same kernels,
         # one CTA per launch), on a stratified sample
         sample = stratified(mols, 48)
+        warm = sg.Molecule.from_geometry(ctx, sample[0])  # first-call set-up stays untimed
+        warm.run(tol=TOL)
+        warm.close()
         tp = time.perf_counter()
         plain_lat = []
         for m in sample:
             t1 = time.perf_counter()
-            sg.Molecule.from_geometry(ctx, m).run(tol=TOL)
+            one = sg.Molecule.from_geometry(ctx, m)
+            one.run(tol=TOL)
+            one.close()
             plain_lat.append(time.perf_counter() - t1)
         plain = len(sample) / (time.perf_counter() - tp)
         # serving: open-loop Poisson arrivals of the same composition, continuous batching over
