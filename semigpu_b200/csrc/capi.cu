@@ -1,5 +1,6 @@
 // C ABI of the engine (include/semigpu_b200.h).  One translation unit: the device tables live
 // in this TU's constant bank, and every kernel is instantiated here.
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -73,6 +74,7 @@ struct sgb_ctx {
   cudaEvent_t joined[kNumClasses] = {};
   int class_threads[kNumClasses] = {};
   int solver = SOLVER_PURIFY;  // SGB_SOLVER_*
+  cublasHandle_t blas = nullptr;  // created on first use (the products of grid purification)
   // optional reusable arena (sgb_ctx_reserve): a batch that fits takes it instead of calling
   // cudaMalloc, and gives it back without cudaFree (which would synchronise the device)
   char* pool = nullptr;
@@ -121,6 +123,7 @@ struct GridWork {
   char* arena = nullptr;
   size_t bytes = 0;
   double *G = nullptr, *Fprev = nullptr, *wq = nullptr, *dval = nullptr, *partial = nullptr;
+  double* X2 = nullptr;  // purification product (G holds X)
   double* scalars = nullptr;  // [0] E_el, [1] E_cc
   int *occ = nullptr, *vir = nullptr, *flag = nullptr, *result = nullptr;
   unsigned long long* worst = nullptr;
@@ -132,6 +135,7 @@ struct sgb_mol {
   sgb_ctx* ctx = nullptr;
   sgb_batch* b = nullptr;
   bool ints_done = false, hcore_done = false, scf_done = false;
+  bool eig_pending = false;  // grid purification: eigenpairs of Fprev computed on first read
   int path = SGB_PATH_AUTO;
   GridWork gw;
 };
@@ -484,8 +488,9 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
   const int64_t n = mol->b->desc[0].nao;
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
-  const size_t oG = take(8 * n * n), oFp = take(8 * n * n), owq = take(8 * (3 * n + 8)),
-               odv = take(8 * n), opart = take(8 * kPartialMax), osc = take(8 * 4),
+  const size_t oG = take(8 * n * n), oFp = take(8 * n * n), oX2 = take(8 * n * n),
+               owq = take(8 * (3 * n + 8)), odv = take(8 * n), opart = take(8 * 2 * kPartialMax),
+               osc = take(8 * 8),
                oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
                owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
   if (ctx->budget && ctx->in_use + off > ctx->budget)
@@ -495,7 +500,8 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
   ctx->in_use += off;
   w.bytes = off;
   char* b = w.arena;
-  w.G = (double*)(b + oG); w.Fprev = (double*)(b + oFp); w.wq = (double*)(b + owq);
+  w.G = (double*)(b + oG); w.Fprev = (double*)(b + oFp); w.X2 = (double*)(b + oX2);
+  w.wq = (double*)(b + owq);
   w.dval = (double*)(b + odv); w.partial = (double*)(b + opart); w.scalars = (double*)(b + osc);
   w.occ = (int*)(b + oocc); w.vir = (int*)(b + ovir); w.flag = (int*)(b + oflag);
   w.result = (int*)(b + ores); w.worst = (unsigned long long*)(b + owst);
@@ -551,6 +557,84 @@ int grid_jacobi(sgb_ctx* ctx, sgb_mol* mol, const int* ga, int na, const int* gb
   return SGB_OK;
 }
 
+// P (packed) from the full F in T by purification (the recursion and limits of purify.cuh);
+// *products = number of products, or -1 when it did not converge (the caller diagonalises).
+int grid_purify(sgb_ctx* ctx, sgb_mol* mol, int* products) {
+  const MolView v = mol_view(mol->b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = v.nao;
+  const int64_t nn = (int64_t)n * n;
+  if (!ctx->blas) {
+    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS)
+      return fail(ctx, SGB_E_CUDA, "cublasCreate failed");
+  }
+  if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS)
+    return fail(ctx, SGB_E_CUDA, "cublasSetStream failed");
+  double* X = w.G;
+  double* sc = w.scalars;  // [2] lo, [3] hi, [4] tr X, [5] ||X||^2
+  const int nbr = grid_blocks(ctx, 32LL * n);
+  k_pur_bounds<<<nbr, kGridThreads, 0, st>>>(n, v.T, w.partial);
+  k_pur_bounds_reduce<<<1, 32, 0, st>>>(w.partial, nbr, sc + 2);
+  const int nb = grid_blocks(ctx, nn);
+  k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial);
+  double t[2];
+  auto sums = [&]() -> int {
+    k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
+    k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nb, nb, sc + 5);
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaMemcpyAsync(t, sc + 4, 16, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return SGB_OK;
+  };
+  int rc = sums();
+  if (rc) return rc;
+  const double one = 1.0, zero = 0.0, n_o = (double)v.nocc;
+  int tail = -1;
+  *products = -1;
+  for (int it = 0; it <= kPurifyMaxIter; ++it) {
+    if (!(fabs(t[0]) < INFINITY) || !(fabs(t[1]) < INFINITY)) return SGB_OK;
+    if (tail < 0 && t[0] - t[1] < kPurifyIdem) tail = kPurifyTail;
+    if (tail == 0) {
+      if (fabs(t[0] - n_o) < kPurifyTraceTol) {
+        k_pur_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, X, v.P);
+        CUDA_TRY(ctx, cudaGetLastError());
+        *products = it;
+      }
+      return SGB_OK;
+    }
+    if (tail > 0) --tail;
+    if (it == kPurifyMaxIter) break;
+    const int sq = fabs(t[1] - n_o) < fabs(2.0 * t[0] - t[1] - n_o);
+    if (cublasDsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &one, X, n, &zero,
+                    w.X2, n) != CUBLAS_STATUS_SUCCESS)
+      return fail(ctx, SGB_E_CUDA, "cublasDsyrk failed (n = %d)", n);
+    k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial);
+    if ((rc = sums())) return rc;
+  }
+  return SGB_OK;
+}
+
+// Eigenpairs of the F saved in Fprev (the last one that produced a density), fully
+// diagonalised from scratch, sorted ascending into eig / T.
+int grid_eigenpairs(sgb_ctx* ctx, sgb_mol* mol) {
+  const MolView v = mol_view(mol->b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = v.nao;
+  k_grid_identity<<<grid_blocks(ctx, (int64_t)n * n), kGridThreads, 0, st>>>(n, mol->b->d_V, w.G, w.Fprev);
+  CUDA_TRY(ctx, cudaGetLastError());
+  int sw = 0, rc;
+  if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
+  if (sw == -2) return fail(ctx, SGB_E_CUDA, "grid barrier timed out in the Jacobi eigensolver");
+  if (sw < 0) return fail(ctx, SGB_E_EIG, "eigenpairs: Jacobi did not converge");
+  k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, mol->b->d_V, w.dval);
+  k_grid_sorted_output<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, w.dval, mol->b->d_V, v.eig, v.T);
+  CUDA_TRY(ctx, cudaGetLastError());
+  mol->eig_pending = false;
+  return SGB_OK;
+}
+
 int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result* res,
              double* energies) {
   int rc = ensure_grid_work(ctx, mol);
@@ -570,47 +654,58 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
   std::vector<double> hist(1, E);
   int steps = 0, conv = 0, status = SGB_OK;
   const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
+  const bool purify = ctx->solver == SOLVER_PURIFY;
+  mol->eig_pending = false;
   while (!conv && steps < max_iter) {
-    if (steps == 0)
-      k_grid_identity<<<grid_blocks(ctx, nn), kGridThreads, 0, st>>>(n, b->d_V, w.G, v.T);
-    else
-      k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, v.T, b->d_V, w.G);
-    CUDA_TRY(ctx, cudaGetLastError());
-    bool full = steps < kFullJacobiSteps || nocc == 0 || nvir == 0;
-    int sw = 0;
-    if (!full) {
-      k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
-      k_grid_split<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, nocc, w.dval, w.occ, w.vir);
-      const bool o_small = nocc <= nvir;
-      if ((rc = grid_jacobi(ctx, mol, o_small ? w.occ : w.vir, o_small ? nocc : nvir,
-                            o_small ? w.vir : w.occ, o_small ? nvir : nocc, kJacobiDoneGapped, &sw)))
-        return rc;
-      if (sw > 0) {
-        k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
-        k_grid_crossing<<<1, 256, 0, st>>>(nocc, nvir, w.dval, w.occ, w.vir, kCrossMargin, w.flag);
-        int cross = 0;
-        CUDA_TRY(ctx, cudaMemcpyAsync(&cross, w.flag, 4, cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(ctx, cudaStreamSynchronize(st));
-        full = cross != 0;
-      }
+    const bool cold = steps == 0 || purify;
+    bool have_p = false;  // P written by purification; a Jacobi eigensolve only if it failed
+    if (purify) {
+      int prod = -1;
+      if ((rc = grid_purify(ctx, mol, &prod))) return rc;
+      have_p = prod >= 0;
     }
-    if (full) {
-      if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
-      if (sw > 0) {
+    if (!have_p) {
+      if (cold)
+        k_grid_identity<<<grid_blocks(ctx, nn), kGridThreads, 0, st>>>(n, b->d_V, w.G, v.T);
+      else
+        k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, v.T, b->d_V, w.G);
+      CUDA_TRY(ctx, cudaGetLastError());
+      bool full = cold || steps < kFullJacobiSteps || nocc == 0 || nvir == 0;
+      int sw = 0;
+      if (!full) {
         k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
         k_grid_split<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, nocc, w.dval, w.occ, w.vir);
+        const bool o_small = nocc <= nvir;
+        if ((rc = grid_jacobi(ctx, mol, o_small ? w.occ : w.vir, o_small ? nocc : nvir,
+                              o_small ? w.vir : w.occ, o_small ? nvir : nocc, kJacobiDoneGapped, &sw)))
+          return rc;
+        if (sw > 0) {
+          k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+          k_grid_crossing<<<1, 256, 0, st>>>(nocc, nvir, w.dval, w.occ, w.vir, kCrossMargin, w.flag);
+          int cross = 0;
+          CUDA_TRY(ctx, cudaMemcpyAsync(&cross, w.flag, 4, cudaMemcpyDeviceToHost, st));
+          CUDA_TRY(ctx, cudaStreamSynchronize(st));
+          full = cross != 0;
+        }
+      }
+      if (full) {
+        if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
+        if (sw > 0) {
+          k_grid_rayleigh<<<grid_blocks(ctx, 32LL * n), kGridThreads, 0, st>>>(n, w.G, b->d_V, w.dval);
+          k_grid_split<<<grid_blocks(ctx, n), kGridThreads, 0, st>>>(n, nocc, w.dval, w.occ, w.vir);
+        }
+      }
+      if (sw == -2) return fail(ctx, SGB_E_CUDA, "grid barrier timed out in the Jacobi eigensolver");
+      if (sw < 0) { status = SGB_E_EIG; break; }
+      if (nocc > 0) {
+        const int tiles = (n + 3) / 4;
+        k_grid_density<<<grid_blocks(ctx, (int64_t)tiles * (tiles + 1) / 2), kGridThreads, 0, st>>>(
+            n, nocc, b->d_V, w.occ, v.P);
+      } else {
+        CUDA_TRY(ctx, cudaMemsetAsync(v.P, 0, 8 * tri(n), st));
       }
     }
-    if (sw == -2) return fail(ctx, SGB_E_CUDA, "grid barrier timed out in the Jacobi eigensolver");
-    if (sw < 0) { status = SGB_E_EIG; break; }
-    if (nocc > 0) {
-      const int tiles = (n + 3) / 4;
-      k_grid_density<<<grid_blocks(ctx, (int64_t)tiles * (tiles + 1) / 2), kGridThreads, 0, st>>>(
-          n, nocc, b->d_V, w.occ, v.P);
-    } else {
-      CUDA_TRY(ctx, cudaMemsetAsync(v.P, 0, 8 * tri(n), st));
-    }
-    // keep the F this eigensolve diagonalised: the final eigenpairs are reported for it
+    // keep the F that produced this density: the final eigenpairs are reported for it
     CUDA_TRY(ctx, cudaMemcpyAsync(w.Fprev, v.T, 8 * nn, cudaMemcpyDeviceToDevice, st));
     if ((rc = grid_fock(ctx, mol, true))) return rc;
     const double Eold = E;
@@ -622,8 +717,11 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
     conv = fabs(Eold - E) < tol;
   }
   // eigenpairs of the last eigensolve's F, fully diagonalised (the loop may have rotated only
-  // occupied-virtual pairs), sorted ascending into eig / T
-  if (steps > 0 && status == SGB_OK) {
+  // occupied-virtual pairs), sorted ascending into eig / T; after purification they are
+  // computed when first read (sgb_get)
+  if (steps > 0 && status == SGB_OK && purify) {
+    mol->eig_pending = true;
+  } else if (steps > 0 && status == SGB_OK) {
     k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, w.Fprev, b->d_V, w.G);
     int sw = 0;
     if ((rc = grid_jacobi(ctx, mol, nullptr, 0, nullptr, 0, kJacobiDoneAbs, &sw))) return rc;
@@ -813,6 +911,7 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
   free_batch(ctx->cached);
   ctx->cached = nullptr;
   if (ctx->pool) cudaFree(ctx->pool);
+  if (ctx->blas) cublasDestroy(ctx->blas);
   for (int k = 0; k < kNumClasses; ++k) {
     if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);
@@ -974,6 +1073,10 @@ int sgb_fock(sgb_ctx* ctx, sgb_mol* mol, const double* P, double* F, double* e_e
 
 int sgb_get(sgb_ctx* ctx, const sgb_mol* mol, int which, double* host, size_t count) {
   if (!ctx || !mol || !host) return SGB_E_ARG;
+  if ((which == SGB_EIGVAL || which == SGB_EIGVEC) && mol->eig_pending) {
+    const int rc = grid_eigenpairs(ctx, const_cast<sgb_mol*>(mol));
+    if (rc) return rc;
+  }
   const sgb_batch* b = mol->b;
   const MolDesc& d = b->desc[0];
   const double* src = nullptr;

@@ -153,6 +153,95 @@ __global__ void k_reduce_sum(const double* partial, int n, double* out) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Purification on the whole GPU: the recursion of purify.cuh for one large molecule.  The
+// products X^2 are symmetric rank-n updates issued by the host loop (cuBLAS DSYRK, lower
+// triangle, column-major); these kernels build X_0, apply the chosen branch and reduce tr X and
+// ||X||_F^2 -- block partials, then one fixed-order pass, so the sums are deterministic.
+
+// Gershgorin bounds: per block, min over its rows of F_ii - r_i and max of F_ii + r_i
+// (partial[2 blk], partial[2 blk + 1]); warp per row.
+__global__ void k_pur_bounds(int n, const double* __restrict__ F, double* partial) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  double lo = INFINITY, hi = -INFINITY;
+  for (int64_t i = (int64_t)blockIdx.x * nwb + wib; i < n; i += (int64_t)gridDim.x * nwb) {
+    const double* row = F + i * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += j == i ? 0.0 : fabs(row[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    lo = fmin(lo, row[i] - s);
+    hi = fmax(hi, row[i] + s);
+  }
+  __shared__ double rlo[32], rhi[32];
+  if (lane == 0) { rlo[wib] = lo; rhi[wib] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nwb; ++k) { lo = fmin(lo, rlo[k]); hi = fmax(hi, rhi[k]); }
+    partial[2 * blockIdx.x] = lo;
+    partial[2 * blockIdx.x + 1] = hi;
+  }
+}
+
+__global__ void k_pur_bounds_reduce(const double* partial, int nb, double* lohi) {
+  if (threadIdx.x == 0) {
+    double lo = INFINITY, hi = -INFINITY;
+    for (int b = 0; b < nb; ++b) { lo = fmin(lo, partial[2 * b]); hi = fmax(hi, partial[2 * b + 1]); }
+    if (!(hi - lo > 1e-12)) hi = lo + 1.0;
+    lohi[0] = lo;
+    lohi[1] = hi;
+  }
+}
+
+// X_0 = (hi I - F) / (hi - lo); block partials of tr X (partial[blk]) and ||X||^2
+// (partial[gridDim + blk]).
+__global__ void k_pur_init(int n, const double* __restrict__ F, const double* lohi, double* X,
+                           double* partial) {
+  const double lo = lohi[0], hi = lohi[1], inv = 1.0 / (hi - lo);
+  const int64_t nn = (int64_t)n * n;
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const int64_t i = t / n, j = t - i * n;
+    const double v = ((i == j ? hi : 0.0) - F[t]) * inv;
+    X[t] = v;
+    if (i == j) s1 += v;
+    s2 = fma(v, v, s2);
+  }
+  write_block_partial(s1, partial);
+  __syncthreads();
+  write_block_partial(s2, partial + gridDim.x);
+}
+
+// X <- X2 (sq) or 2X - X2 on the lower triangle of X2 (column-major), mirrored; partial sums
+// of the new tr X and ||X||^2 as in k_pur_init.
+__global__ void k_pur_update(int n, double* X, const double* __restrict__ X2, int sq,
+                             double* partial) {
+  const int64_t nn = (int64_t)n * n;
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const int64_t j = t / n, i = t - j * n;  // element (i, j) at i + j n
+    if (i < j) continue;
+    const double x2 = X2[t];
+    const double v = sq ? x2 : fma(2.0, X[t], -x2);
+    X[t] = v;
+    if (i != j) X[j + i * n] = v;
+    if (i == j) s1 += v;
+    s2 = fma(i == j ? v : 2.0 * v, v, s2);
+  }
+  write_block_partial(s1, partial);
+  __syncthreads();
+  write_block_partial(s2, partial + gridDim.x);
+}
+
+// P (packed lower triangle) = 2 X
+__global__ void k_pur_density(int n, const double* X, double* P) {
+  for (int64_t t = gtid(); t < tri(n); t += gstride()) {
+    int i, j;
+    tri_inverse(t, i, j);
+    P[t] = 2.0 * X[(int64_t)i * n + j];
+  }
+}
+
+// ------------------------------------------------------------------------------------------
 // Dense pieces of the eigensolve (column-major n x n, ld n)
 
 __global__ void k_grid_identity(int n, double* V, double* G, const double* F) {
