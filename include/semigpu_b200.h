@@ -66,11 +66,16 @@ const char *sgb_status_string(int status);
  *   SGB_SOLVER_PURIFY (default) -- trace-correcting purification on the FP64 tensor-core path
  *     for nao <= 160 (the same aufbau projector; a Jacobi eigensolve replaces it for a step
  *     where it does not converge, and gives the eigenpairs at the end of sgb_scf);
- *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step.
+ *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step;
+ *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: for one large molecule (the grid path,
+ *     nao > 160) the purification products run in FP32 until the recursion is near idempotent
+ *     and finish in FP64 (Fock, energies and the convergence test stay FP64); the one-CTA path
+ *     keeps FP64 products.
  * Molecules above nao 160 always diagonalise.  The environment variable
- * SGB_DENSITY_SOLVER=jacobi changes the default (also for sgb_scf_noalloc). */
+ * SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for sgb_scf_noalloc). */
 #define SGB_SOLVER_PURIFY 0
 #define SGB_SOLVER_JACOBI 1
+#define SGB_SOLVER_PURIFY_MIXED 2
 int sgb_ctx_set_density_solver(sgb_ctx *ctx, int solver);
 /* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
  * it instead of allocating, and releasing the batch does not free device memory (cudaFree

@@ -25,7 +25,7 @@ OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN = (
     0, -1, -2, -3, -4, -5, -6, 1, 2)
 BLOCKS, HCORE, FOCK, DENSITY, EIGVAL, EIGVEC = range(6)
 PATH_AUTO, PATH_CTA, PATH_GRID = range(3)
-SOLVER_PURIFY, SOLVER_JACOBI = range(2)
+SOLVER_PURIFY, SOLVER_JACOBI, SOLVER_PURIFY_MIXED = range(3)
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -146,7 +146,8 @@ class Context:
         self.check(lib().sgb_ctx_synchronize(self.h), "synchronize")
 
     def set_density_solver(self, solver: int):
-        """SOLVER_PURIFY (default) or SOLVER_JACOBI for the SCF steps of later calls."""
+        """SOLVER_PURIFY (default), SOLVER_JACOBI or SOLVER_PURIFY_MIXED for the SCF steps of
+        later calls."""
         self.check(lib().sgb_ctx_set_density_solver(self.h, int(solver)), "set_density_solver")
 
     def reserve(self, nbytes: int):

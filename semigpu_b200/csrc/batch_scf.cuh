@@ -97,7 +97,10 @@ enum : int { STAGE_INTS = 1, STAGE_HCORE = 2, STAGE_SCF = 4, STAGE_CC = 8, STAGE
 
 enum : int { MOL_OK = 0, MOL_EIG_FAILED = 1, MOL_NAN = 2 };
 
-enum : int { SOLVER_PURIFY = 0, SOLVER_JACOBI = 1 };
+// SOLVER_PURIFY_MIXED: as SOLVER_PURIFY, with the products of the grid path (one large
+// molecule) in FP32 until the recursion is near idempotent, FP64 after; the one-CTA path keeps
+// FP64 products.
+enum : int { SOLVER_PURIFY = 0, SOLVER_JACOBI = 1, SOLVER_PURIFY_MIXED = 2 };
 
 __host__ __device__ inline int smem_ld(int n) { return n | 1; }
 
@@ -281,7 +284,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
-    const bool purify = PLACE != 2 && a.solver == SOLVER_PURIFY;
+    const bool purify = PLACE != 2 && a.solver != SOLVER_JACOBI;
     while (!conv && steps < a.max_iter) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {

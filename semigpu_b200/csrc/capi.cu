@@ -39,10 +39,12 @@ constexpr SizeClass kClasses[] = {{32, 2, 128},  {64, 2, 256},   {96, 3, 512},  
 constexpr int kNumClasses = 7;
 constexpr int kBatchScfMax = 1024;  // one CTA per molecule up to here; the grid path above
 
-// SGB_SOLVER_PURIFY unless the environment sets SGB_DENSITY_SOLVER=jacobi.
+// SGB_SOLVER_PURIFY unless the environment sets SGB_DENSITY_SOLVER=jacobi or =mixed.
 int default_solver() {
   const char* env = getenv("SGB_DENSITY_SOLVER");
-  return env && strcmp(env, "jacobi") == 0 ? SOLVER_JACOBI : SOLVER_PURIFY;
+  if (env && strcmp(env, "jacobi") == 0) return SOLVER_JACOBI;
+  if (env && strcmp(env, "mixed") == 0) return SOLVER_PURIFY_MIXED;
+  return SOLVER_PURIFY;
 }
 
 int class_of(int nao) {
@@ -559,7 +561,11 @@ int grid_jacobi(sgb_ctx* ctx, sgb_mol* mol, const int* ga, int na, const int* gb
 
 // P (packed) from the full F in T by purification (the recursion and limits of purify.cuh);
 // *products = number of products, or -1 when it did not converge (the caller diagonalises).
-int grid_purify(sgb_ctx* ctx, sgb_mol* mol, int* products) {
+// mixed: X and the products in FP32 (SSYRK) while tr(X - X^2) >= kPurifyMixedSwitch, then X is
+// widened to FP64 and the recursion finishes with FP64 products, so the result carries FP64
+// idempotency; the FP32 phase only perturbs the occupied subspace at the 1e-7 level, which
+// enters the energy at second order.
+int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   const MolView v = mol_view(mol->b);
   GridWork& w = mol->gw;
   cudaStream_t st = ctx->stream;
@@ -577,7 +583,13 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, int* products) {
   k_pur_bounds<<<nbr, kGridThreads, 0, st>>>(n, v.T, w.partial);
   k_pur_bounds_reduce<<<1, 32, 0, st>>>(w.partial, nbr, sc + 2);
   const int nb = grid_blocks(ctx, nn);
-  k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial);
+  float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
+  float* Y32 = X32 + nn;
+  bool fp32 = mixed;
+  if (fp32)
+    k_pur_init32<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X32, w.partial);
+  else
+    k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial);
   double t[2];
   auto sums = [&]() -> int {
     k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
@@ -590,10 +602,16 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, int* products) {
   int rc = sums();
   if (rc) return rc;
   const double one = 1.0, zero = 0.0, n_o = (double)v.nocc;
+  const float onef = 1.0f, zerof = 0.0f;
   int tail = -1;
   *products = -1;
   for (int it = 0; it <= kPurifyMaxIter; ++it) {
     if (!(fabs(t[0]) < INFINITY) || !(fabs(t[1]) < INFINITY)) return SGB_OK;
+    if (fp32 && t[0] - t[1] < kPurifyMixedSwitch) {
+      k_pur_widen<<<nb, kGridThreads, 0, st>>>(nn, X32, X, n, w.partial);
+      if ((rc = sums())) return rc;
+      fp32 = false;
+    }
     if (tail < 0 && t[0] - t[1] < kPurifyIdem) tail = kPurifyTail;
     if (tail == 0) {
       if (fabs(t[0] - n_o) < kPurifyTraceTol) {
@@ -606,10 +624,17 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, int* products) {
     if (tail > 0) --tail;
     if (it == kPurifyMaxIter) break;
     const int sq = fabs(t[1] - n_o) < fabs(2.0 * t[0] - t[1] - n_o);
-    if (cublasDsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &one, X, n, &zero,
-                    w.X2, n) != CUBLAS_STATUS_SUCCESS)
-      return fail(ctx, SGB_E_CUDA, "cublasDsyrk failed (n = %d)", n);
-    k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial);
+    if (fp32) {
+      if (cublasSsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &onef, X32, n, &zerof,
+                      Y32, n) != CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, SGB_E_CUDA, "cublasSsyrk failed (n = %d)", n);
+      k_pur_update32<<<nb, kGridThreads, 0, st>>>(n, X32, Y32, sq, w.partial);
+    } else {
+      if (cublasDsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &one, X, n, &zero,
+                      w.X2, n) != CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, SGB_E_CUDA, "cublasDsyrk failed (n = %d)", n);
+      k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial);
+    }
     if ((rc = sums())) return rc;
   }
   return SGB_OK;
@@ -654,14 +679,14 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
   std::vector<double> hist(1, E);
   int steps = 0, conv = 0, status = SGB_OK;
   const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
-  const bool purify = ctx->solver == SOLVER_PURIFY;
+  const bool purify = ctx->solver != SOLVER_JACOBI;
   mol->eig_pending = false;
   while (!conv && steps < max_iter) {
     const bool cold = steps == 0 || purify;
     bool have_p = false;  // P written by purification; a Jacobi eigensolve only if it failed
     if (purify) {
       int prod = -1;
-      if ((rc = grid_purify(ctx, mol, &prod))) return rc;
+      if ((rc = grid_purify(ctx, mol, ctx->solver == SOLVER_PURIFY_MIXED, &prod))) return rc;
       have_p = prod >= 0;
     }
     if (!have_p) {
@@ -876,9 +901,12 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
 
 int sgb_ctx_set_density_solver(sgb_ctx* ctx, int solver) {
   if (!ctx) return SGB_E_ARG;
-  if (solver != SGB_SOLVER_PURIFY && solver != SGB_SOLVER_JACOBI)
+  if (solver != SGB_SOLVER_PURIFY && solver != SGB_SOLVER_JACOBI &&
+      solver != SGB_SOLVER_PURIFY_MIXED)
     return fail(ctx, SGB_E_ARG, "unknown density solver %d", solver);
-  ctx->solver = solver == SGB_SOLVER_JACOBI ? SOLVER_JACOBI : SOLVER_PURIFY;
+  ctx->solver = solver == SGB_SOLVER_JACOBI         ? SOLVER_JACOBI
+                : solver == SGB_SOLVER_PURIFY_MIXED ? SOLVER_PURIFY_MIXED
+                                                    : SOLVER_PURIFY;
   return SGB_OK;
 }
 

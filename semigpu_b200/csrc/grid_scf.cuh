@@ -232,6 +232,58 @@ __global__ void k_pur_update(int n, double* X, const double* __restrict__ X2, in
   write_block_partial(s2, partial + gridDim.x);
 }
 
+// Mixed precision: the same two kernels on an FP32 X (products on the tensor cores as
+// split-BF16 FP32 emulation); the sums stay FP64.
+__global__ void k_pur_init32(int n, const double* __restrict__ F, const double* lohi, float* X,
+                             double* partial) {
+  const double lo = lohi[0], hi = lohi[1], inv = 1.0 / (hi - lo);
+  const int64_t nn = (int64_t)n * n;
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const int64_t i = t / n, j = t - i * n;
+    const float v = (float)(((i == j ? hi : 0.0) - F[t]) * inv);
+    X[t] = v;
+    if (i == j) s1 += v;
+    s2 = fma((double)v, (double)v, s2);
+  }
+  write_block_partial(s1, partial);
+  __syncthreads();
+  write_block_partial(s2, partial + gridDim.x);
+}
+
+__global__ void k_pur_update32(int n, float* X, const float* __restrict__ X2, int sq,
+                               double* partial) {
+  const int64_t nn = (int64_t)n * n;
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const int64_t j = t / n, i = t - j * n;
+    if (i < j) continue;
+    const float x2 = X2[t];
+    const float v = sq ? x2 : fmaf(2.0f, X[t], -x2);
+    X[t] = v;
+    if (i != j) X[j + i * n] = v;
+    if (i == j) s1 += v;
+    s2 = fma(i == j ? (double)v : 2.0 * v, (double)v, s2);
+  }
+  write_block_partial(s1, partial);
+  __syncthreads();
+  write_block_partial(s2, partial + gridDim.x);
+}
+
+// FP32 X -> FP64 X for the refinement products, with its sums.
+__global__ void k_pur_widen(int64_t nn, const float* X32, double* X, int n, double* partial) {
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const double v = (double)X32[t];
+    X[t] = v;
+    if (t / n == t % n) s1 += v;
+    s2 = fma(v, v, s2);
+  }
+  write_block_partial(s1, partial);
+  __syncthreads();
+  write_block_partial(s2, partial + gridDim.x);
+}
+
 // P (packed lower triangle) = 2 X
 __global__ void k_pur_density(int n, const double* X, double* P) {
   for (int64_t t = gtid(); t < tri(n); t += gstride()) {

@@ -33,6 +33,8 @@ constexpr double kPurifyIdem = 1e-8;
 constexpr int kPurifyTail = 2;
 constexpr double kPurifyTraceTol = 1e-6;
 constexpr int kPurifyMaxN16 = 160;  // largest padded order held in one CTA's shared memory
+// Mixed precision (grid path): FP32 products until tr(X - X^2) falls below this, FP64 after.
+constexpr double kPurifyMixedSwitch = 1e-3;
 
 __host__ __device__ inline int purify_n16(int n) { return (n + 15) & ~15; }
 __host__ __device__ inline int purify_ld(int n) { return purify_n16(n) + 4; }

@@ -87,3 +87,32 @@ def test_zero_gap_falls_back_to_jacobi(gpu_ctx):
     assert r["status"][0] == 0
     assert np.isfinite(r["E_el"][0])
     assert sc[0, sg.Batch.STAGES.index("full_solves")] >= 1
+
+
+def test_grid_path_purification_matches_jacobi(gpu_ctx, jacobi_ctx):
+    """One large molecule on the whole GPU: purification (DSYRK products) against the Jacobi
+    eigensolver, then its eigenpairs (computed when first read) against the Jacobi ones."""
+    mol = geo.alkane(40, np.random.default_rng(8))  # nao 242
+    a = sg.Molecule.from_geometry(gpu_ctx, mol)
+    b = sg.Molecule.from_geometry(jacobi_ctx, mol)
+    ra, rb = a.run(tol=1e-6), b.run(tol=1e-6)
+    assert ra["n_iter"] == rb["n_iter"]
+    assert abs(ra["E_tot"] - rb["E_tot"]) < 1e-8
+    np.testing.assert_allclose(a.get(sg.DENSITY), b.get(sg.DENSITY), rtol=0, atol=1e-9)
+    np.testing.assert_allclose(a.get(sg.EIGVAL), b.get(sg.EIGVAL), rtol=0, atol=1e-8)
+
+
+def test_mixed_precision_within_tolerance(gpu_ctx, oracle_mod):
+    """Mixed form (FP32 products, FP64 finish) on C100H202 against the FP64 oracle:
+    |dE_total| <= 1e-4 eV (the stated tolerance of the mixed form)."""
+    mol = geo.alkane_c2(0)
+    ctx = sg.Context(0)
+    ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+    try:
+        r = sg.Molecule.from_geometry(ctx, mol).run(tol=1e-6)
+    finally:
+        ctx.close()
+    o = oracle_mod.scf(mol.Z, mol.xyz, tol=1e-6)
+    assert r["converged"] and r["status"] == 0
+    assert abs(r["E_tot"] - o["E_tot"]) <= 1e-4
+    assert abs(r["n_iter"] - o["n_iter"]) <= 1
