@@ -289,7 +289,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {
         // ---- P from F by purification; a Jacobi eigensolve if that fails ----
-        const int prod = block_purify<NT>(Ffull, n, m.nocc, smem, red);
+        const int prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
         clk.lap(ST_PURIFY);
         clk.add(ST_PURIFY_PRODUCTS, (unsigned long long)(prod > 0 ? prod : 0));
         if (prod >= 0) {
