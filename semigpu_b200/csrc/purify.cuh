@@ -45,7 +45,7 @@ constexpr double kPurifyMixedSwitch = 1e-3;
 // and held the whole spectrum on every one of them.  Should an eigenvalue still fall outside,
 // its trace and idempotency checks fail and the step is diagonalised instead.
 constexpr int kLanczosSteps = 8;
-constexpr int kLanczosMinN = 64;
+constexpr int kLanczosMinN = 32;
 constexpr double kLanczosMargin = 1.0;  // eV
 
 // Deterministic start vector with entries in [0.5, 1.5) (not normalised): no symmetry of the
