@@ -11,13 +11,14 @@
 // The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
 // repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
 // max_iter steps.  Two ways to get P from F, chosen per launch:
-//  * SOLVER_PURIFY (default, nao <= 160): P by trace-correcting purification, ~20 symmetric
-//    matrix squares on the FP64 tensor-core path (purify.cuh); a Jacobi eigensolve replaces it
-//    for a step whose purification fails (vanishing gap), and runs once at the end when the
-//    eigenpairs are wanted (single-molecule calls).
+//  * SOLVER_PURIFY (default): P by trace-correcting purification, ~20 symmetric matrix
+//    squares on the FP64 tensor-core path (purify.cuh; X in shared memory up to nao 160, in
+//    global memory above); a Jacobi eigensolve replaces it for a step whose purification fails
+//    (vanishing gap), and runs once at the end when the eigenpairs are wanted (single-molecule
+//    calls).
 //  * SOLVER_JACOBI: a cyclic Jacobi on V^T F V carried on the columns of V and G = F V; after
 //    the first step it is warm-started from the previous eigenvectors, which the new F barely
-//    mixes, so it needs few sweeps.  Molecules above nao 160 always take this one.
+//    mixes, so it needs few sweeps.
 #pragma once
 #include "fock_block.cuh"
 #include "purify.cuh"
@@ -284,16 +285,25 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
-    const bool purify = PLACE != 2 && a.solver != SOLVER_JACOBI;
+    const bool purify = a.solver != SOLVER_JACOBI;
     while (!conv && steps < a.max_iter) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {
         // ---- P from F by purification; a Jacobi eigensolve if that fails ----
-        const int prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
+        int prod;
+        const double* Xr = smem;
+        if constexpr (PLACE == 2) {  // X and its partner in the global work matrix
+          double* Xo = nullptr;
+          prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq, red,
+                                         &Xo);
+          Xr = Xo;
+        } else {
+          prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
+        }
         clk.lap(ST_PURIFY);
         clk.add(ST_PURIFY_PRODUCTS, (unsigned long long)(prod > 0 ? prod : 0));
         if (prod >= 0) {
-          purify_density(smem, n, m.P);
+          purify_density(Xr, n, m.P);
           __syncthreads();
           clk.lap(ST_DENSITY);
         } else {

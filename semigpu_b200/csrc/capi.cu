@@ -235,7 +235,10 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     d.sq0 = sq0;
     d.ao0 = ao0;
     d.w0 = w0;
-    if (nao > kGsmemMax) w0 += ((int64_t)nao * nao + 31) / 32 * 32;
+    if (nao > kGsmemMax) {  // Jacobi's G (n x n) or purification's X and Y
+      const int64_t need = std::max<int64_t>((int64_t)nao * nao, 2 * (int64_t)purify_doubles(nao));
+      w0 += (need + 31) / 32 * 32;
+    }
     blk0 += (roff + 31) / 32 * 32;
     pk0 += (tri(nao) + 31) / 32 * 32;
     sq0 += ((int64_t)nao * nao + 31) / 32 * 32;

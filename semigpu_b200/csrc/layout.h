@@ -25,7 +25,7 @@ struct MolDesc {
   int64_t sq0;    // first double of its square matrices
   int64_t ao0;    // first entry of its per-AO vectors
   int64_t nblk;   // integral doubles owned
-  int64_t w0;     // first double of its eigensolver work matrix in global memory (nao > 160)
+  int64_t w0;     // first double of its work matrices in global memory (nao > 160)
 };
 
 // Block offset (relative to the molecule's blk0) of atom pair (A, B), A >= B.

@@ -395,6 +395,100 @@ __device__ int block_purify(const double* F, int n, int nocc, double* X, double*
   return -1;
 }
 
+// Above nao 160 X does not fit in shared memory: X and Y (n16 x n16, row stride n16 + 4) live
+// in global memory (L1/L2-resident panels).  A warp takes one super-tile at a time, keeps its
+// four 8 x 8 accumulators in registers and writes the new values straight into Y, reading the
+// old X for the 2X - X^2 branch; the caller swaps X and Y after each step.
+template <int NT>
+__device__ __noinline__ void purify_step_global(const double* __restrict__ X,
+                                                double* __restrict__ Y, int n16, int ld, bool sq,
+                                                double* red, int buf, double& t1, double& t2) {
+  constexpr int NW = NT / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane >> 2, q = lane & 3;
+  const int nst = n16 >> 4, cnt = nst * (nst + 1) / 2;
+  double s1 = 0.0, s2 = 0.0;
+  int I = 0, J = 0;
+  if (warp < cnt) tri_inverse(warp, I, J);
+  for (int st = warp; st < cnt; st += NW) {
+    const int64_t ri = (int64_t)(I * 16 + g) * ld + q, rj = (int64_t)(J * 16 + g) * ld + q;
+    double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+    const bool diag = I == J;
+    for (int k0 = 0; k0 < n16; k0 += 4) {
+      const double a0 = X[ri + k0], a1 = X[ri + 8 * ld + k0];
+      const double b0 = X[rj + k0], b1 = X[rj + 8 * ld + k0];
+      dmma884(acc[0][0], acc[0][1], a0, b0);
+      if (!diag) dmma884(acc[1][0], acc[1][1], a0, b1);
+      dmma884(acc[2][0], acc[2][1], a1, b0);
+      dmma884(acc[3][0], acc[3][1], a1, b1);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = I * 16 + (k >> 1) * 8 + g;
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int c = J * 16 + (k & 1) * 8 + 2 * q + e;
+        if (r >= c) {
+          const double x2 = acc[k][e];
+          const double v = sq ? x2 : fma(2.0, X[(int64_t)r * ld + c], -x2);
+          Y[(int64_t)r * ld + c] = v;
+          if (r != c) Y[(int64_t)c * ld + r] = v;
+          if (r == c) s1 += v;
+          s2 = fma(r == c ? v : 2.0 * v, v, s2);
+        }
+      }
+    }
+    // next super-tile of this warp: advance the packed index by NW
+    J += NW;
+    while (J > I) { J -= I + 1; ++I; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  double* part = red + 32 * buf;
+  if (lane == 0) { part[warp] = s1; part[16 + warp] = s2; }
+  __syncthreads();  // Y and the partial sums complete
+  s1 = 0.0;
+  s2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < NW; ++k) { s1 += part[k]; s2 += part[16 + k]; }
+  t1 = s1;
+  t2 = s2;
+}
+
+// block_purify with X and its partner Y in global memory (nao > 160).  Returns the number of
+// products and leaves the result in *Xout (X or Y), or -1.
+template <int NT>
+__device__ int block_purify_global(const double* F, int n, int nocc, double* X, double* Y,
+                                   double* lz, double* red, double** Xout) {
+  const int ld = purify_ld(n), n16 = purify_n16(n);
+  double t1, t2;
+  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+  // Y's padding must be zero as X's is: the steps only write the n16 x n16 block
+  for (int64_t t = threadIdx.x; t < (int64_t)n16 * ld; t += NT) Y[t] = 0.0;
+  __syncthreads();
+  int tail = -1;
+  for (int it = 0; it <= kPurifyMaxIter; ++it) {
+    if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) return -1;
+    if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+    if (tail == 0) {
+      *Xout = X;
+      return fabs(t1 - (double)nocc) < kPurifyTraceTol ? it : -1;
+    }
+    if (tail > 0) --tail;
+    if (it == kPurifyMaxIter) break;
+    const double n_o = (double)nocc;
+    const bool sq = fabs(t2 - n_o) < fabs(2.0 * t1 - t2 - n_o);
+    purify_step_global<NT>(X, Y, n16, ld, sq, red, it & 1, t1, t2);
+    double* tmp = X;
+    X = Y;
+    Y = tmp;
+  }
+  return -1;
+}
+
 // P (packed lower triangle) = 2 X.
 __device__ inline void purify_density(const double* X, int n, double* P) {
   const int ld = purify_ld(n);

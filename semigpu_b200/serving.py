@@ -31,13 +31,17 @@ SMEM_MAX_NAO = 160  # above this a batched molecule also holds an n x n eigensol
 
 def device_bytes(mol: Geometry) -> int:
     """Device memory a molecule occupies inside a batch (integral blocks, Hcore/P/F packed,
-    eigenvectors + F full square (+ the work matrix above nao 160), eigenvalues, atom arrays)."""
+    eigenvectors + F full square (+ the work matrices above nao 160), eigenvalues, atom
+    arrays)."""
     heavy = int(np.count_nonzero(mol.Z > 1))
     light = mol.natoms - heavy
     nblk = 100 * heavy * (heavy + 1) // 2 + 10 * heavy * light + light * (light + 1) // 2
     n = mol.nao
-    squares = 3 if n > SMEM_MAX_NAO else 2
-    return 8 * (nblk + 3 * n * (n + 1) // 2 + squares * n * n + n) + 64 * mol.natoms + 256
+    squares = 2 * n * n
+    if n > SMEM_MAX_NAO:  # work matrices X and Y of purification, n16 x (n16 + 4) each
+        n16 = (n + 15) // 16 * 16
+        squares += max(n * n, 2 * n16 * (n16 + 4))
+    return 8 * (nblk + 3 * n * (n + 1) // 2 + squares + n) + 64 * mol.natoms + 256
 
 
 @dataclass
