@@ -2,13 +2,17 @@
 
 A `Server` owns `slots` workers on one GPU.  Each worker has its own engine context (its own
 CUDA streams), so the persistent launches of different workers run concurrently on the device.
-A free worker takes every request waiting in the queue -- up to `max_batch` molecules and up to
+A free worker takes every request waiting in its queue -- up to `max_batch` molecules and up to
 its share of the HBM budget, by each molecule's device footprint -- builds one device batch
-(integrals, Hcore, P, F, eigenvectors stay resident for the whole SCF) and runs it; requests
-that arrive meanwhile wait for the next free worker, so batches form continuously from whatever
-has arrived (continuous batching at launch granularity).  Molecules up to nao 1024 share the
-batch (one CTA each); larger ones run through the single-molecule grid path in the worker that
-picked them.
+(integrals, Hcore, P, F, density stay resident for the whole SCF) and runs it; requests that
+arrive meanwhile wait for the next free worker, so batches form continuously from whatever has
+arrived (continuous batching at launch granularity).
+
+Requests are queued by size: molecules up to nao 160 (SCF matrices in shared memory, a few ms)
+and larger ones (up to nao 1024 in the batch, seconds at the top of the range) have separate
+queues, and `big_slots` of the workers serve only the large queue, so a small request never
+waits for a batch that holds a large molecule.  Molecules above nao 1024 run through the
+single-molecule grid path in the large-queue worker that picked them.
 
 Latency of a request = completion time - arrival time (host clock); `stats()` reports p50/p99
 and throughput.  `replay()` drives an open-loop arrival schedule (e.g. Poisson) in real time.
@@ -26,7 +30,7 @@ from . import Context, Molecule, run_molecules
 from .geometry import Molecule as Geometry
 
 CTA_MAX_NAO = 1024  # larger molecules take the grid path
-SMEM_MAX_NAO = 160  # above this a batched molecule also holds an n x n eigensolver work matrix
+SMEM_MAX_NAO = 160  # above this a batched molecule also holds its work matrices in global memory
 
 
 def device_bytes(mol: Geometry) -> int:
@@ -57,22 +61,25 @@ class Request:
 class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
-                 batch_window_s: float = 0.0, engine=None):
+                 batch_window_s: float = 0.0, engine=None, big_slots: int = 1):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
-        replaceable for host-only tests of the scheduling."""
+        replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
+        queue of molecules above nao 160 (at least one slot stays with the small queue)."""
         self.tol, self.max_iter = tol, max_iter
         self.max_batch = max_batch
         self.slot_budget = hbm_budget // max(1, slots)
         self.window = batch_window_s
         self.engine = engine or run_molecules
-        self._queue: collections.deque[Request] = collections.deque()
+        self._queues = (collections.deque(), collections.deque())  # small, large
+        self.big_slots = max(0, min(big_slots, slots - 1))
         self._cv = threading.Condition()
         self._done: list[Request] = []
         self._next = 0
         self._stop = False
         self._device = device
-        self._workers = [threading.Thread(target=self._work, args=(i,), daemon=True)
-                         for i in range(slots)]
+        # the last big_slots workers serve the large queue
+        self._workers = [threading.Thread(target=self._work, args=(i, i >= slots - self.big_slots),
+                                          daemon=True) for i in range(slots)]
         self.batches: list[tuple[int, int, float, float]] = []  # (worker, size, t0, t1)
         self._errors: list[BaseException] = []
         for w in self._workers:
@@ -83,8 +90,9 @@ class Server:
         with self._cv:
             rid = self._next
             self._next += 1
-            self._queue.append(Request(rid, mol, time.perf_counter() if t_arrival is None else t_arrival))
-            self._cv.notify()
+            req = Request(rid, mol, time.perf_counter() if t_arrival is None else t_arrival)
+            self._queues[int(self.big_slots > 0 and mol.nao > SMEM_MAX_NAO)].append(req)
+            self._cv.notify_all()
         return rid
 
     def drain(self, timeout: float = 600.0) -> list[Request]:
@@ -118,18 +126,20 @@ class Server:
         return self.drain()
 
     # -- worker side ------------------------------------------------------------------------
-    def _take(self) -> list[Request]:
-        """Everything waiting, up to max_batch molecules and this worker's HBM share."""
+    def _take(self, queue) -> list[Request]:
+        """Everything waiting in `queue`, up to max_batch molecules and this worker's HBM
+        share."""
         out, used = [], 0
-        while self._queue and len(out) < self.max_batch:
-            need = device_bytes(self._queue[0].mol)
+        while queue and len(out) < self.max_batch:
+            need = device_bytes(queue[0].mol)
             if out and used + need > self.slot_budget:
                 break
             used += need
-            out.append(self._queue.popleft())
+            out.append(queue.popleft())
         return out
 
-    def _work(self, idx: int):
+    def _work(self, idx: int, big: bool = False):
+        queue = self._queues[int(big)]
         ctx = None
         try:
             if self.engine is run_molecules:
@@ -139,14 +149,14 @@ class Server:
                 ctx.reserve(self.slot_budget + (64 << 20))
             while True:
                 with self._cv:
-                    while not self._queue and not self._stop:
+                    while not queue and not self._stop:
                         self._cv.wait(0.05)
-                    if self._stop and not self._queue:
+                    if self._stop and not queue:
                         return
                 if self.window:
                     time.sleep(self.window)
                 with self._cv:
-                    reqs = self._take()
+                    reqs = self._take(queue)
                 if not reqs:
                     continue
                 t0 = time.perf_counter()

@@ -43,6 +43,34 @@ def test_every_request_answered_once_with_its_own_result():
     assert len(log) < 300  # requests were batched
 
 
+def test_small_and_large_molecules_never_share_a_batch():
+    """Molecules above nao 160 have their own queue and worker: a small request is never held
+    in a batch with a large one."""
+    batches = []
+    lock = threading.Lock()
+    inner = _fake_engine(delay=0.003)
+
+    def engine(ctx, mols, tol, max_iter):
+        with lock:
+            batches.append([m.nao for m in mols])
+        return inner(ctx, mols, tol, max_iter)
+
+    rng = np.random.default_rng(4)
+    mols = geo.batch_c3(120, seed=6) + [geo.alkane(int(k), rng) for k in (30, 45, 60, 80)]
+    order = rng.permutation(len(mols))
+    srv = serving.Server(slots=3, big_slots=1, engine=engine)
+    try:
+        for i in order:
+            srv.submit(mols[i])
+        done = srv.drain(timeout=60)
+    finally:
+        srv.close()
+    assert len(done) == len(mols)
+    for b in batches:
+        assert all(n > serving.SMEM_MAX_NAO for n in b) or all(n <= serving.SMEM_MAX_NAO for n in b)
+    assert any(all(n > serving.SMEM_MAX_NAO for n in b) for b in batches)
+
+
 def test_admission_respects_hbm_share():
     log = []
     mols = geo.batch_c3(50, seed=3)
