@@ -77,6 +77,11 @@ const char *sgb_status_string(int status);
 #define SGB_SOLVER_JACOBI 1
 #define SGB_SOLVER_PURIFY_MIXED 2
 int sgb_ctx_set_density_solver(sgb_ctx *ctx, int solver);
+/* Caps the batched launches of this context at share x (number of SMs) CTAs' worth of SMs
+ * (0 < share <= 1; 1 = the whole GPU, the default).  No counterpart in the reference; a
+ * server running several contexts side by side uses it so that one context's persistent
+ * launch of long (large-molecule) work leaves SMs to the others. */
+int sgb_ctx_set_sm_share(sgb_ctx *ctx, double share);
 /* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
  * it instead of allocating, and releasing the batch does not free device memory (cudaFree
  * synchronises the whole device, which would stall other contexts' work).  One batch at a time

@@ -41,6 +41,7 @@ SIGNATURES = {
     "sgb_ctx_bytes_in_use": (ctypes.c_size_t, [_VP]),
     "sgb_ctx_reserve": (ctypes.c_int, [_VP, ctypes.c_size_t]),
     "sgb_ctx_set_density_solver": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sgb_ctx_set_sm_share": (ctypes.c_int, [_VP, ctypes.c_double]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_heat_of_formation": (ctypes.c_int, [ctypes.c_int, _I, ctypes.c_double, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
@@ -149,6 +150,10 @@ class Context:
         """SOLVER_PURIFY (default), SOLVER_JACOBI or SOLVER_PURIFY_MIXED for the SCF steps of
         later calls."""
         self.check(lib().sgb_ctx_set_density_solver(self.h, int(solver)), "set_density_solver")
+
+    def set_sm_share(self, share: float):
+        """Batched launches of this context use at most this fraction of the SMs."""
+        self.check(lib().sgb_ctx_set_sm_share(self.h, float(share)), "set_sm_share")
 
     def reserve(self, nbytes: int):
         """Reusable device arena for batches of up to `nbytes` (see sgb_ctx_reserve)."""

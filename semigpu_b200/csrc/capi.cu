@@ -76,7 +76,13 @@ struct sgb_ctx {
   cudaEvent_t joined[kNumClasses] = {};
   int class_threads[kNumClasses] = {};
   int solver = SOLVER_PURIFY;  // SGB_SOLVER_*
+  int sm_limit = 0;            // batched launches use at most this many SMs' worth of CTAs (0: all)
   cublasHandle_t blas = nullptr;  // created on first use (the products of grid purification)
+  // Timing events for batches, created with the context and recycled: cudaEventCreate waits
+  // for the kernels running on the device, which would stall a batch built while another
+  // context's long launch runs.
+  std::vector<cudaEvent_t> events;
+  std::mutex events_mutex;
   // optional reusable arena (sgb_ctx_reserve): a batch that fits takes it instead of calling
   // cudaMalloc, and gives it back without cudaFree (which would synchronise the device)
   char* pool = nullptr;
@@ -171,6 +177,28 @@ size_t align_up(size_t x) { return (x + kAlign - 1) / kAlign * kAlign; }
 // Estimated SCF cost used to order the persistent launch (largest first).
 double cost_of(const MolDesc& d) { return (double)d.nao * d.nao * d.nao + 50.0 * d.natoms * d.natoms; }
 
+cudaError_t take_event(sgb_ctx* ctx, cudaEvent_t* ev) {
+  {
+    std::lock_guard<std::mutex> lock(ctx->events_mutex);
+    if (!ctx->events.empty()) {
+      *ev = ctx->events.back();
+      ctx->events.pop_back();
+      return cudaSuccess;
+    }
+  }
+  return cudaEventCreate(ev);
+}
+
+void give_event(sgb_ctx* ctx, cudaEvent_t ev) {
+  if (!ev) return;
+  if (!ctx) {
+    cudaEventDestroy(ev);
+    return;
+  }
+  std::lock_guard<std::mutex> lock(ctx->events_mutex);
+  ctx->events.push_back(ev);
+}
+
 void free_batch(sgb_batch* b) {
   if (!b) return;
   if (b->arena && b->from_pool) {
@@ -179,8 +207,8 @@ void free_batch(sgb_batch* b) {
     cudaFree(b->arena);
     if (b->ctx) b->ctx->in_use -= b->bytes;
   }
-  if (b->ev0) cudaEventDestroy(b->ev0);
-  if (b->ev1) cudaEventDestroy(b->ev1);
+  give_event(b->ctx, b->ev0);
+  give_event(b->ctx, b->ev1);
   delete b;
 }
 
@@ -337,7 +365,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
       (e = up(b->d_row_off, row_off.data(), 8 * NA)) != cudaSuccess ||
       (e = up(b->d_hb, hb.data(), 4 * NA)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->d_status, 0, 4 * nmol, st)) != cudaSuccess ||
-      (e = cudaEventCreate(&b->ev0)) != cudaSuccess || (e = cudaEventCreate(&b->ev1)) != cudaSuccess) {
+      (e = take_event(ctx, &b->ev0)) != cudaSuccess || (e = take_event(ctx, &b->ev1)) != cudaSuccess) {
     free_batch(b);
     return cuda_fail(ctx, e, "batch upload");
   }
@@ -353,21 +381,58 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
 
 // One kernel instantiation per (threads per CTA, eigenvector column registers per lane).
 // The dynamic shared memory cap is a per-function attribute shared by every host thread and
-// context, so it is always raised to the device's opt-in maximum (never to a launch's own size,
-// which another thread could lower between its set and its launch).
+// context, so it is raised to the device's opt-in maximum (never to a launch's own size, which
+// another thread could lower between its set and its launch), and only once per device:
+// setting it waits for the kernels running on the device, which would stall one context's
+// launch behind another's long persistent launch.
+constexpr int kMaxDevices = 64;
+
+// Raises the kernel's cap on the current device (once); *cap receives it.
+template <int NT, int CR>
+cudaError_t kernel_smem_cap(int* cap) {
+  auto* k = k_batch_scf<NT, CR>;
+  static int max_dynamic[kMaxDevices] = {};  // 0: not set yet on that device
+  static std::mutex set_mutex;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(set_mutex);
+  if (!max_dynamic[dev]) {
+    int optin = 0;
+    cudaFuncAttributes fa;
+    if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess ||
+        (e = cudaFuncGetAttributes(&fa, k)) != cudaSuccess)
+      return e;
+    const int md = optin - (int)fa.sharedSizeBytes;  // the static part counts against it
+    if ((e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, md)) != cudaSuccess)
+      return e;
+    max_dynamic[dev] = md;
+  }
+  *cap = max_dynamic[dev];
+  return cudaSuccess;
+}
+
+// Every instantiation, at context creation (before any long launch can be running).
+cudaError_t prepare_kernels() {
+  int c = 0;
+  cudaError_t e;
+  if ((e = kernel_smem_cap<512, 0>(&c)) || (e = kernel_smem_cap<128, 2>(&c)) ||
+      (e = kernel_smem_cap<256, 2>(&c)) || (e = kernel_smem_cap<256, 3>(&c)) ||
+      (e = kernel_smem_cap<256, 4>(&c)) || (e = kernel_smem_cap<256, 5>(&c)) ||
+      (e = kernel_smem_cap<512, 2>(&c)) || (e = kernel_smem_cap<512, 3>(&c)) ||
+      (e = kernel_smem_cap<512, 4>(&c)) || (e = kernel_smem_cap<512, 5>(&c)))
+    return e;
+  return cudaSuccess;
+}
+
 template <int NT, int CR>
 cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStream_t st) {
   auto* k = k_batch_scf<NT, CR>;
-  int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  cudaFuncAttributes fa;
-  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k);
+  int cap = 0;
+  cudaError_t e = kernel_smem_cap<NT, CR>(&cap);
   if (e != cudaSuccess) return e;
-  const int max_dynamic = optin - (int)fa.sharedSizeBytes;  // the static part counts against it
-  if (smem > (size_t)max_dynamic) return cudaErrorInvalidValue;
-  e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic);
-  if (e != cudaSuccess) return e;
+  if (smem > (size_t)cap) return cudaErrorInvalidValue;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, smem);
   if (e != cudaSuccess) return e;
@@ -449,7 +514,8 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
     const size_t smem = (ac.mat_doubles + extra_doubles(ac.nmax)) * sizeof(double);
     cudaStream_t cs = ctx->aux[c];
     CUDA_TRY(ctx, cudaStreamWaitEvent(cs, b->ev0, 0));
-    cudaError_t e = launch_class(ctx->num_sms, ac, kClasses[c].cr, ctx->class_threads[c], smem, cs);
+    const int sms = ctx->sm_limit > 0 ? std::min(ctx->sm_limit, ctx->num_sms) : ctx->num_sms;
+    cudaError_t e = launch_class(sms, ac, kClasses[c].cr, ctx->class_threads[c], smem, cs);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "k_batch_scf launch");
     CUDA_TRY(ctx, cudaEventRecord(ctx->joined[c], cs));
     CUDA_TRY(ctx, cudaStreamWaitEvent(st, ctx->joined[c], 0));
@@ -562,6 +628,53 @@ int grid_jacobi(sgb_ctx* ctx, sgb_mol* mol, const int* ga, int na, const int* gb
   return SGB_OK;
 }
 
+// Lanczos-refined bounds (purify.cuh) for the F in T, intersected with the Gershgorin ones
+// already in lohi[0..1] (device).  Worth its host round trips only for large n, where one
+// product costs milliseconds.
+constexpr int kGridLanczosMinN = 1536;
+
+int grid_lanczos_bounds(sgb_ctx* ctx, sgb_mol* mol, double* lohi) {
+  const MolView v = mol_view(mol->b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = v.nao;
+  double* q = w.X2;  // free until the first product
+  double* qp = q + n;
+  double* wv = qp + n;
+  double* sc = w.scalars;
+  const int nb = grid_blocks(ctx, n);
+  k_lz_start<<<nb, kGridThreads, 0, st>>>(n, q, qp, w.partial);
+  k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 6);
+  k_lz_scale<<<nb, kGridThreads, 0, st>>>(n, q, sc + 6);
+  const int nbr = grid_blocks(ctx, 32LL * n);
+  double al[kLanczosSteps], be[kLanczosSteps], beta = 0.0, h[2];
+  for (int k = 0; k < kLanczosSteps; ++k) {
+    k_lz_matvec<<<nbr, kGridThreads, 0, st>>>(n, v.T, q, qp, beta, wv, w.partial);
+    k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nbr, sc + 6);
+    k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nbr, nbr, sc + 7);
+    CUDA_TRY(ctx, cudaGetLastError());
+    CUDA_TRY(ctx, cudaMemcpyAsync(h, sc + 6, 16, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    const double alpha = h[0], nbv = sqrt(std::max(h[1] - alpha * alpha, 0.0));
+    al[k] = alpha;
+    be[k] = nbv;
+    if (!(nbv > 1e-10 * (fabs(alpha) + 1.0))) return SGB_OK;  // invariant subspace: keep Gershgorin
+    k_lz_update<<<nb, kGridThreads, 0, st>>>(n, q, qp, wv, alpha, 1.0 / nbv);
+    beta = nbv;
+  }
+  double g[2];
+  CUDA_TRY(ctx, cudaMemcpyAsync(g, lohi, 16, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  double llo, lhi;
+  lanczos_bounds<kLanczosSteps>(al, be, be[kLanczosSteps - 1], llo, lhi);
+  if (llo == llo && lhi == lhi) {
+    g[0] = std::max(g[0], llo);
+    g[1] = std::min(g[1], lhi);
+    CUDA_TRY(ctx, cudaMemcpy(lohi, g, 16, cudaMemcpyHostToDevice));
+  }
+  return SGB_OK;
+}
+
 // P (packed) from the full F in T by purification (the recursion and limits of purify.cuh);
 // *products = number of products, or -1 when it did not converge (the caller diagonalises).
 // mixed: X and the products in FP32 (SSYRK) while tr(X - X^2) >= kPurifyMixedSwitch, then X is
@@ -585,6 +698,10 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   const int nbr = grid_blocks(ctx, 32LL * n);
   k_pur_bounds<<<nbr, kGridThreads, 0, st>>>(n, v.T, w.partial);
   k_pur_bounds_reduce<<<1, 32, 0, st>>>(w.partial, nbr, sc + 2);
+  if (n >= kGridLanczosMinN) {
+    int rc = grid_lanczos_bounds(ctx, mol, sc + 2);
+    if (rc) return rc;
+  }
   const int nb = grid_blocks(ctx, nn);
   float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
   float* Y32 = X32 + nn;
@@ -872,7 +989,7 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   c->budget = budget;
   if ((e = cudaSetDevice(device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = upload_tables()) != cudaSuccess ||
+      (e = upload_tables()) != cudaSuccess || (e = prepare_kernels()) != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
     delete c;
     return SGB_E_CUDA;
@@ -880,6 +997,14 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   c->smem_optin = optin;
+  for (int k = 0; k < 8; ++k) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) {
+      sgb_ctx_destroy(c);
+      return SGB_E_CUDA;
+    }
+    c->events.push_back(ev);
+  }
   for (int k = 0; k < kNumClasses; ++k) {
     c->class_threads[k] = kClasses[k].threads;
     if (cudaStreamCreateWithFlags(&c->aux[k], cudaStreamNonBlocking) != cudaSuccess ||
@@ -910,6 +1035,12 @@ int sgb_ctx_set_density_solver(sgb_ctx* ctx, int solver) {
   ctx->solver = solver == SGB_SOLVER_JACOBI         ? SOLVER_JACOBI
                 : solver == SGB_SOLVER_PURIFY_MIXED ? SOLVER_PURIFY_MIXED
                                                     : SOLVER_PURIFY;
+  return SGB_OK;
+}
+
+int sgb_ctx_set_sm_share(sgb_ctx* ctx, double share) {
+  if (!ctx || !(share > 0.0) || share > 1.0) return SGB_E_ARG;
+  ctx->sm_limit = share >= 1.0 ? 0 : std::max(1, (int)(share * ctx->num_sms));
   return SGB_OK;
 }
 
@@ -948,6 +1079,7 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
     if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);
   }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
   delete ctx;
   return SGB_OK;
 }
@@ -1291,7 +1423,7 @@ int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!nd.ready) {
       void* ptr = nullptr;
-      if (upload_tables() != cudaSuccess) return SGB_E_CUDA;
+      if (upload_tables() != cudaSuccess || prepare_kernels() != cudaSuccess) return SGB_E_CUDA;
       if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return SGB_E_CUDA;
       if (cudaDeviceGetAttribute(&nd.num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return SGB_E_CUDA;

@@ -284,6 +284,56 @@ __global__ void k_pur_widen(int64_t nn, const float* X32, double* X, int n, doub
   write_block_partial(s2, partial + gridDim.x);
 }
 
+// Lanczos steps of the spectral bounds (purify.cuh), for one large molecule: the host keeps
+// the coefficients and the loop; vectors q, q_prev, w of length n on the device.
+__global__ void k_lz_start(int n, double* q, double* qp, double* partial) {
+  double s = 0.0;
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double v = lanczos_start((int)i);
+    q[i] = v;
+    qp[i] = 0.0;
+    s = fma(v, v, s);
+  }
+  write_block_partial(s, partial);
+}
+
+__global__ void k_lz_scale(int n, double* q, const double* sumsq) {
+  const double inv = 1.0 / sqrt(*sumsq);
+  for (int64_t i = gtid(); i < n; i += gstride()) q[i] *= inv;
+}
+
+// w = F q - beta q_prev (warp per row); block partials of q.w and w.w
+__global__ void k_lz_matvec(int n, const double* __restrict__ F, const double* q,
+                            const double* qp, double beta, double* w, double* partial) {
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  double qw = 0.0, ww = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * nwb + wib; i < n; i += (int64_t)gridDim.x * nwb) {
+    const double* row = F + i * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s = fma(row[j], q[j], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const double wi = s - beta * qp[i];
+    if (lane == 0) {
+      w[i] = wi;
+      qw = fma(q[i], wi, qw);
+      ww = fma(wi, wi, ww);
+    }
+  }
+  write_block_partial(qw, partial);
+  __syncthreads();
+  write_block_partial(ww, partial + gridDim.x);
+}
+
+__global__ void k_lz_update(int n, double* q, double* qp, const double* w, double alpha,
+                            double rnb) {
+  for (int64_t i = gtid(); i < n; i += gstride()) {
+    const double qi = q[i];
+    qp[i] = qi;
+    q[i] = (w[i] - alpha * qi) * rnb;
+  }
+}
+
 // P (packed lower triangle) = 2 X
 __global__ void k_pur_density(int n, const double* X, double* P) {
   for (int64_t t = gtid(); t < tri(n); t += gstride()) {

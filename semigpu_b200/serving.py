@@ -61,10 +61,14 @@ class Request:
 class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
-                 batch_window_s: float = 0.0, engine=None, big_slots: int = 1):
+                 batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
+                 big_sm_share: float = 0.6):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
-        queue of molecules above nao 160 (at least one slot stays with the small queue)."""
+        queue of molecules above nao 160 (at least one slot stays with the small queue); their
+        launches together use at most big_sm_share of the SMs, so the persistent large-molecule
+        launches (seconds) always leave SMs to the small ones."""
+        self.big_sm_share = big_sm_share
         self.tol, self.max_iter = tol, max_iter
         self.max_batch = max_batch
         self.slot_budget = hbm_budget // max(1, slots)
@@ -144,6 +148,8 @@ class Server:
         try:
             if self.engine is run_molecules:
                 ctx = Context(self._device)
+                if big and self.big_slots:
+                    ctx.set_sm_share(max(0.05, self.big_sm_share / self.big_slots))
                 # batches are built in a per-worker arena: no cudaMalloc/cudaFree per batch
                 # (cudaFree would synchronise the device and stall the other workers)
                 ctx.reserve(self.slot_budget + (64 << 20))
@@ -207,3 +213,53 @@ def stats(done: list[Request]) -> dict:
             "p99_ms": 1e3 * float(np.percentile(lat, 99)),
             "molecules_per_s": len(done) / (t_last - t_first) if t_last > t_first else float("nan"),
             "all_converged": bool(all(r.result.get("converged", False) for r in done))}
+
+
+def main(argv=None):
+    """Replays seeded open-loop Poisson arrivals and prints latency and throughput, overall and
+    for the small (nao <= 160) and large molecules:
+
+        python -m semigpu_b200.serving --workload c5 --rate 2000 --duration 3
+    """
+    import argparse
+    import json
+
+    from . import geometry as geo
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--workload", choices=["c3", "c5"], default="c5",
+                    help="c3: the 4096-batch composition; c5: alkanes extended to C150H302")
+    ap.add_argument("--rate", type=float, default=2000.0, help="requests per second")
+    ap.add_argument("--duration", type=float, default=3.0, help="seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--big-slots", type=int, default=2)
+    ap.add_argument("--hbm-gb", type=float, default=40.0)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    if args.workload == "c5":
+        arrivals = geo.serving_c5(rate=args.rate, duration_s=args.duration, seed=args.seed)
+    else:
+        rng = np.random.default_rng(args.seed + 1)
+        t, times = 0.0, []
+        while True:
+            t += rng.exponential(1.0 / args.rate)
+            if t >= args.duration:
+                break
+            times.append(t)
+        arrivals = list(zip(times, geo.batch_c3(len(times), seed=args.seed)))
+    srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)))
+    try:
+        srv.replay([(0.001 * i, m) for i, (_, m) in enumerate(arrivals[:40])])  # warm-up
+        done = srv.replay(arrivals)
+    finally:
+        srv.close()
+    out = {"workload": args.workload, "rate_per_s": args.rate, "duration_s": args.duration,
+           "all": stats(done),
+           "small": stats([r for r in done if r.mol.nao <= SMEM_MAX_NAO]),
+           "large": stats([r for r in done if r.mol.nao > SMEM_MAX_NAO]),
+           "max_nao": max(r.mol.nao for r in done)}
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
