@@ -42,6 +42,7 @@ SIGNATURES = {
     "sgb_ctx_reserve": (ctypes.c_int, [_VP, ctypes.c_size_t]),
     "sgb_ctx_set_density_solver": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_ctx_set_sm_share": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "sgb_ctx_set_diis": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_heat_of_formation": (ctypes.c_int, [ctypes.c_int, _I, ctypes.c_double, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
@@ -150,6 +151,10 @@ class Context:
         """SOLVER_PURIFY (default), SOLVER_JACOBI or SOLVER_PURIFY_MIXED for the SCF steps of
         later calls."""
         self.check(lib().sgb_ctx_set_density_solver(self.h, int(solver)), "set_density_solver")
+
+    def set_diis(self, depth: int):
+        """Pulay DIIS of this depth (0 = off) for single-molecule runs on the grid path."""
+        self.check(lib().sgb_ctx_set_diis(self.h, int(depth)), "set_diis")
 
     def set_sm_share(self, share: float):
         """Batched launches of this context use at most this fraction of the SMs."""

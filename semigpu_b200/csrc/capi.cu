@@ -77,6 +77,7 @@ struct sgb_ctx {
   int class_threads[kNumClasses] = {};
   int solver = SOLVER_PURIFY;  // SGB_SOLVER_*
   int sm_limit = 0;            // batched launches use at most this many SMs' worth of CTAs (0: all)
+  int diis = 0;                // DIIS depth of the grid-path SCF (0: off)
   cublasHandle_t blas = nullptr;  // created on first use (the products of grid purification)
   // Timing events for batches, created with the context and recycled: cudaEventCreate waits
   // for the kernels running on the device, which would stall a batch built while another
@@ -132,6 +133,10 @@ struct GridWork {
   size_t bytes = 0;
   double *G = nullptr, *Fprev = nullptr, *wq = nullptr, *dval = nullptr, *partial = nullptr;
   double* X2 = nullptr;  // purification product (G holds X)
+  // DIIS history (grid path, when enabled): depth x (F, error) n x n pairs, and the B matrix
+  double* diis = nullptr;
+  int diis_cap = 0;
+  size_t diis_bytes = 0;
   double* scalars = nullptr;  // [0] E_el, [1] E_cc
   int *occ = nullptr, *vir = nullptr, *flag = nullptr, *result = nullptr;
   unsigned long long* worst = nullptr;
@@ -561,7 +566,7 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
   auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
   const size_t oG = take(8 * n * n), oFp = take(8 * n * n), oX2 = take(8 * n * n),
                owq = take(8 * (3 * n + 8)), odv = take(8 * n), opart = take(8 * 2 * kPartialMax),
-               osc = take(8 * 8),
+               osc = take(8 * 16),
                oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
                owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
   if (ctx->budget && ctx->in_use + off > ctx->budget)
@@ -581,6 +586,10 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
 }
 
 void free_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
+  if (mol->gw.diis) {
+    cudaFree(mol->gw.diis);
+    if (ctx) ctx->in_use -= mol->gw.diis_bytes;
+  }
   if (mol->gw.arena) {
     cudaFree(mol->gw.arena);
     if (ctx) ctx->in_use -= mol->gw.bytes;
@@ -780,6 +789,93 @@ int grid_eigenpairs(sgb_ctx* ctx, sgb_mol* mol) {
   return SGB_OK;
 }
 
+// Pulay DIIS for the grid path (optional; changes the SCF trajectory, so off by default).
+// After the Fock build of step k, with X = P_k / 2 still in G: store F_k and e_k = F_k P_k -
+// P_k F_k, extend B_ij = <e_i, e_j>, solve [B 1; 1^T 0][c; l] = [0; 1] on the host and write
+// F = sum c_i F_i into T for the next density.  The reported energy stays that of F_k.
+struct DiisState {
+  int depth = 0, count = 0, next = 0;
+  double B[8][8] = {};
+};
+
+int diis_step(sgb_ctx* ctx, sgb_mol* mol, DiisState& ds) {
+  const MolView v = mol_view(mol->b);
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int n = v.nao, depth = ds.depth;
+  const int64_t nn = (int64_t)n * n;
+  if (w.diis_cap < depth) {
+    if (w.diis) {
+      cudaFree(w.diis);
+      ctx->in_use -= w.diis_bytes;
+      w.diis = nullptr;
+    }
+    const size_t bytes = 2 * (size_t)depth * nn * 8;
+    if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+      return fail(ctx, SGB_E_NOMEM, "DIIS history needs %zu bytes over the budget", bytes);
+    if (cudaMalloc(&w.diis, bytes) != cudaSuccess) return fail(ctx, SGB_E_NOMEM, "DIIS history");
+    ctx->in_use += bytes;
+    w.diis_bytes = bytes;
+    w.diis_cap = depth;
+  }
+  double* Fh = w.diis;               // depth F matrices
+  double* Eh = w.diis + depth * nn;  // depth error matrices
+  const int slot = ds.next;
+  CUDA_TRY(ctx, cudaMemcpyAsync(Fh + slot * nn, v.T, 8 * nn, cudaMemcpyDeviceToDevice, st));
+  const double two = 2.0, zero = 0.0;  // C = F (2X) = F P
+  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &two, v.T, n, w.G, n, &zero,
+                  w.X2, n) != CUBLAS_STATUS_SUCCESS)
+    return fail(ctx, SGB_E_CUDA, "cublasDgemm failed (DIIS error)");
+  const int nb = grid_blocks(ctx, nn);
+  k_commutator<<<nb, kGridThreads, 0, st>>>(n, w.X2, Eh + slot * nn);
+  ds.count = std::min(ds.count + 1, depth);
+  ds.next = (slot + 1) % depth;
+  for (int j = 0; j < ds.count; ++j) {
+    k_dot<<<nb, kGridThreads, 0, st>>>(nn, Eh + slot * nn, Eh + j * nn, w.partial);
+    k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, w.scalars + 8 + j);
+  }
+  CUDA_TRY(ctx, cudaGetLastError());
+  double row[8];
+  CUDA_TRY(ctx, cudaMemcpyAsync(row, w.scalars + 8, 8 * ds.count, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  for (int j = 0; j < ds.count; ++j) ds.B[slot][j] = ds.B[j][slot] = row[j];
+  const int m = ds.count;
+  if (m < 2) return SGB_OK;
+  // [B 1; 1 0] c = [0; 1], Gaussian elimination with partial pivoting (m <= 8), scaled by
+  // the largest diagonal entry
+  double scale = 0.0;
+  for (int i = 0; i < m; ++i) scale = std::max(scale, ds.B[i][i]);
+  if (!(scale > 0.0)) return SGB_OK;
+  double A[9][10] = {};
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) A[i][j] = ds.B[i][j] / scale;
+    A[i][m] = A[m][i] = 1.0;
+  }
+  A[m][m + 1] = 1.0;
+  for (int c = 0; c <= m; ++c) {
+    int piv = c;
+    for (int r = c + 1; r <= m; ++r)
+      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+    if (!(fabs(A[piv][c]) > 1e-14)) return SGB_OK;  // singular: keep F_k
+    for (int k = 0; k <= m + 1; ++k) std::swap(A[c][k], A[piv][k]);
+    for (int r = 0; r <= m; ++r) {
+      if (r == c) continue;
+      const double f = A[r][c] / A[c][c];
+      for (int k = c; k <= m + 1; ++k) A[r][k] -= f * A[c][k];
+    }
+  }
+  LinComb lc;
+  lc.m = m;
+  for (int i = 0; i < m; ++i) {
+    lc.src[i] = Fh + i * nn;
+    lc.c[i] = A[i][m + 1] / A[i][i];
+    if (!(fabs(lc.c[i]) < 1e6)) return SGB_OK;
+  }
+  k_lincomb<<<nb, kGridThreads, 0, st>>>(nn, lc, v.T);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return SGB_OK;
+}
+
 int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_result* res,
              double* energies) {
   int rc = ensure_grid_work(ctx, mol);
@@ -801,6 +897,8 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
   const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
   const bool purify = ctx->solver != SOLVER_JACOBI;
   mol->eig_pending = false;
+  DiisState ds;
+  ds.depth = purify ? ctx->diis : 0;
   while (!conv && steps < max_iter) {
     const bool cold = steps == 0 || purify;
     bool have_p = false;  // P written by purification; a Jacobi eigensolve only if it failed
@@ -860,6 +958,7 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
     hist.push_back(E);
     if (E != E) { status = SGB_E_NAN; break; }
     conv = fabs(Eold - E) < tol;
+    if (!conv && ds.depth > 0 && have_p && (rc = diis_step(ctx, mol, ds))) return rc;
   }
   // eigenpairs of the last eigensolve's F, fully diagonalised (the loop may have rotated only
   // occupied-virtual pairs), sorted ascending into eig / T; after purification they are
@@ -1035,6 +1134,12 @@ int sgb_ctx_set_density_solver(sgb_ctx* ctx, int solver) {
   ctx->solver = solver == SGB_SOLVER_JACOBI         ? SOLVER_JACOBI
                 : solver == SGB_SOLVER_PURIFY_MIXED ? SOLVER_PURIFY_MIXED
                                                     : SOLVER_PURIFY;
+  return SGB_OK;
+}
+
+int sgb_ctx_set_diis(sgb_ctx* ctx, int depth) {
+  if (!ctx || depth < 0 || depth > 8 || depth == 1) return SGB_E_ARG;
+  ctx->diis = depth;
   return SGB_OK;
 }
 

@@ -334,6 +334,37 @@ __global__ void k_lz_update(int n, double* q, double* qp, const double* w, doubl
   }
 }
 
+// DIIS on the grid path (off by default): the error of step k is the commutator
+// F_k P_k - P_k F_k (the basis is orthonormal in NDDO), formed from C = F P as C - C^T.
+__global__ void k_commutator(int n, const double* __restrict__ C, double* E) {
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    const int64_t j = t / n, i = t - j * n;
+    E[t] = C[t] - C[j + i * n];
+  }
+}
+
+__global__ void k_dot(int64_t nn, const double* __restrict__ a, const double* __restrict__ b,
+                      double* partial) {
+  double s = 0.0;
+  for (int64_t t = gtid(); t < nn; t += gstride()) s = fma(a[t], b[t], s);
+  write_block_partial(s, partial);
+}
+
+struct LinComb {
+  const double* src[8];
+  double c[8];
+  int m;
+};
+
+__global__ void k_lincomb(int64_t nn, LinComb lc, double* out) {
+  for (int64_t t = gtid(); t < nn; t += gstride()) {
+    double v = 0.0;
+    for (int k = 0; k < lc.m; ++k) v = fma(lc.c[k], lc.src[k][t], v);
+    out[t] = v;
+  }
+}
+
 // P (packed lower triangle) = 2 X
 __global__ void k_pur_density(int n, const double* X, double* P) {
   for (int64_t t = gtid(); t < tri(n); t += gstride()) {

@@ -116,3 +116,19 @@ def test_mixed_precision_within_tolerance(gpu_ctx, oracle_mod):
     assert r["converged"] and r["status"] == 0
     assert abs(r["E_tot"] - o["E_tot"]) <= 1e-4
     assert abs(r["n_iter"] - o["n_iter"]) <= 1
+
+
+def test_diis_converges_to_the_same_energy_in_no_more_steps():
+    """Optional DIIS on the grid path: same converged energy as the reference's plain loop
+    (within its tolerance), and no more steps."""
+    mol = geo.polyene(60, np.random.default_rng(12))  # nao 302, conjugated: slow plain SCF
+    ctx = sg.Context(0)
+    try:
+        plain = sg.Molecule.from_geometry(ctx, mol).run(tol=1e-6, max_iter=100)
+        ctx.set_diis(6)
+        diis = sg.Molecule.from_geometry(ctx, mol).run(tol=1e-6, max_iter=100)
+    finally:
+        ctx.close()
+    assert plain["converged"] and diis["converged"]
+    assert diis["n_iter"] <= plain["n_iter"]
+    assert abs(diis["E_tot"] - plain["E_tot"]) < 1e-5
