@@ -146,47 +146,72 @@ __device__ __noinline__ double fock_xx_blocks(const MolView& m, const int* hv, i
   return e;
 }
 
+// Writes F(i, j) = h - g / 2 of an off-diagonal block (h, p preloaded); returns p (h + F).
+__device__ __forceinline__ double put_offdiag_h(double* __restrict__ F, double* Fs, int ld, int i,
+                                                int j, double p, double g, double h) {
+  const double fv = h - 0.5 * g;
+  F[tri(i) + j] = fv;
+  if (Fs) {
+    Fs[(int64_t)i * ld + j] = fv;
+    Fs[(int64_t)j * ld + i] = fv;
+  }
+  return p * (h + fv);
+}
+
 // Blocks of atom A with a hydrogen in them: those of its row (B <= A) and of its column
 // (rows A2 > A), one block per lane.  Writes A's Coulomb sums over them into J; returns the
-// energy share of the row's off-diagonal blocks.
+// energy share of the row's off-diagonal blocks.  All of a block's loads (integrals, P and H
+// entries) are issued before its arithmetic; the restrict-qualified locals let the compiler
+// keep them ahead of the previous block's stores.
 __device__ __noinline__ double fock_atom_light(const MolView& m, int A, const double* wq,
                                                double* J, double* Fs, int ld) {
   const int lane = threadIdx.x & 31;
   const int na = m.natoms;
-  const int fA = m.first[A];
-  const double* row = m.ints + m.row_off[A];
+  const double* __restrict__ ints = m.ints;
+  const double* __restrict__ P = m.P;
+  const double* __restrict__ H = m.H;
+  double* __restrict__ F = m.F;
+  const int8_t* __restrict__ slot = m.slot;
+  const int* __restrict__ first = m.first;
+  const int* __restrict__ hb = m.hb;
+  const int64_t* __restrict__ row_off = m.row_off;
+  const int fA = first[A];
+  const double* row = ints + row_off[A];
   double e = 0.0;
-  if (m.slot[A] != 0) {
+  if (slot[A] != 0) {
     double jl[10];
 #pragma unroll
     for (int r = 0; r < 10; ++r) jl[r] = 0.0;
     // row A, hydrogen B < A: 10 values (pq_A | s_B s_B)
     for (int B = lane; B < A; B += 32) {
-      if (m.slot[B] != 0) continue;
-      const double* I = row + row_block(m, true, B);
-      double Iv[10];
+      if (slot[B] != 0) continue;
+      const int h_ = hb[B], fB = first[B];
+      const double* I = row + (int64_t)h_ * 100 + (int64_t)(B - h_) * 10;
+      double Iv[10], pl[4], hl[4];
 #pragma unroll
       for (int r = 0; r < 10; ++r) Iv[r] = I[r];
-      const double w = wq[wq_offset(m, B)];
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        pl[l] = P[tri(fA + l) + fB];
+        hl[l] = H[tri(fA + l) + fB];
+      }
+      const double w = wq[9 * h_ + B];
 #pragma unroll
       for (int r = 0; r < 10; ++r) jl[r] = fma(Iv[r], w, jl[r]);
-      const int fB = m.first[B];
-      double pl[4];
-#pragma unroll
-      for (int l = 0; l < 4; ++l) pl[l] = m.P[tri(fA + l) + fB];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         double g = 0.0;
 #pragma unroll
         for (int l = 0; l < 4; ++l) g = fma(pl[l], Iv[pair_index(u, l)], g);
-        e += put_offdiag(m, Fs, ld, fA + u, fB, pl[u], g);
+        e += put_offdiag_h(F, Fs, ld, fA + u, fB, pl[u], g, hl[u]);
       }
     }
     // column A, hydrogen rows A2 > A: 10 values (s_A2 s_A2 | q_A)
+    const int hA = hb[A];
     for (int A2 = A + 1 + lane; A2 < na; A2 += 32) {
-      if (m.slot[A2] != 0) continue;
-      const double* I = m.ints + m.row_off[A2] + row_block(m, false, A);
-      const double w = wq[wq_offset(m, A2)];
+      if (slot[A2] != 0) continue;
+      const double* I = ints + row_off[A2] + (int64_t)hA * 10 + (A - hA);
+      const double w = wq[9 * hb[A2] + A2];
 #pragma unroll
       for (int r = 0; r < 10; ++r) jl[r] = fma(I[r], w, jl[r]);
     }
@@ -196,60 +221,66 @@ __device__ __noinline__ double fock_atom_light(const MolView& m, int A, const do
       const double v = warp_sum(jl[r]);
       if (lane == r) mine = v;
     }
-    if (lane < 10) J[wq_offset(m, A) + lane] = mine;
+    if (lane < 10) J[9 * hA + A + lane] = mine;
   } else {
     double jr = 0.0;
     // row A: every B <= A
     for (int B = lane; B <= A; B += 32) {
-      const double* I = row + row_block(m, false, B);
-      const int fB = m.first[B];
-      if (m.slot[B] != 0) {  // 10 values (s_A s_A | q_B)
-        double Iv[10];
+      const int h_ = hb[B], fB = first[B];
+      const double* I = row + (int64_t)h_ * 10 + (B - h_);
+      if (slot[B] != 0) {  // 10 values (s_A s_A | q_B)
+        double Iv[10], ps[4], hs[4];
 #pragma unroll
         for (int q = 0; q < 10; ++q) Iv[q] = I[q];
-        const double* wB = wq + wq_offset(m, B);
+#pragma unroll
+        for (int s_ = 0; s_ < 4; ++s_) {
+          ps[s_] = P[tri(fA) + fB + s_];
+          hs[s_] = H[tri(fA) + fB + s_];
+        }
+        const double* wB = wq + 9 * h_ + B;
 #pragma unroll
         for (int q = 0; q < 10; ++q) jr = fma(Iv[q], wB[q], jr);
-        double ps[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) ps[s] = m.P[tri(fA) + fB + s];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
           double g = 0.0;
 #pragma unroll
-          for (int s = 0; s < 4; ++s) g = fma(ps[s], Iv[pair_index(v, s)], g);
-          e += put_offdiag(m, Fs, ld, fA, fB + v, ps[v], g);
+          for (int s_ = 0; s_ < 4; ++s_) g = fma(ps[s_], Iv[pair_index(v, s_)], g);
+          e += put_offdiag_h(F, Fs, ld, fA, fB + v, ps[v], g, hs[v]);
         }
       } else {
         const double I0 = I[0];
-        jr = fma(I0, wq[wq_offset(m, B)], jr);
+        jr = fma(I0, wq[9 * h_ + B], jr);
         if (B < A) {
-          const double p = m.P[tri(fA) + fB];
-          e += put_offdiag(m, Fs, ld, fA, fB, p, p * I0);
+          const int64_t ij = tri(fA) + fB;
+          const double p = P[ij], h = H[ij];
+          e += put_offdiag_h(F, Fs, ld, fA, fB, p, p * I0, h);
         }
       }
     }
     // column A: every row A2 > A
+    const int hA = hb[A];
     for (int A2 = A + 1 + lane; A2 < na; A2 += 32) {
-      const bool h2 = m.slot[A2] != 0;
-      const double* I = m.ints + m.row_off[A2] + row_block(m, h2, A);
-      const double* w2 = wq + wq_offset(m, A2);
+      const bool h2 = slot[A2] != 0;
+      const double* I = ints + row_off[A2] + (h2 ? (int64_t)hA * 100 + (int64_t)(A - hA) * 10
+                                                 : (int64_t)hA * 10 + (A - hA));
+      const double* w2 = wq + 9 * hb[A2] + A2;
       if (h2) {
-        double s = 0.0;
+        double s_ = 0.0;
 #pragma unroll
-        for (int r = 0; r < 10; ++r) s = fma(I[r], w2[r], s);
-        jr += s;
+        for (int r = 0; r < 10; ++r) s_ = fma(I[r], w2[r], s_);
+        jr += s_;
       } else {
         jr = fma(I[0], w2[0], jr);
       }
     }
     jr = warp_sum(jr);
-    if (lane == 0) J[wq_offset(m, A)] = jr;
+    if (lane == 0) J[9 * hA + A] = jr;
   }
   return e;
 }
 
-// Diagonal block element (A, pq): H + J - 1/2 one-center exchange; its share of E_el.
+// Diagonal block element (A, pq): H + J - 1/2 one-center exchange; its share of E_el.  The
+// atom's P block and the heavy-heavy partial sums are read before the arithmetic.
 __device__ __forceinline__ double fock_diag_final(const MolView& m, const double* J,
                                                   const double* xs, int nh, double* Fs, int ld,
                                                   int t) {
@@ -257,21 +288,31 @@ __device__ __forceinline__ double fock_diag_final(const MolView& m, const double
   const int sA = m.slot[A];
   if (sA == 0 && pq) return 0.0;
   const int a = pair_first(pq), b = pair_second(pq), fA = m.first[A];
-  double K = 0.0;
   const int nA = nao_of_slot(sA);
-  for (int l = 0; l < nA; ++l)
-    for (int s = 0; s < nA; ++s) {
-      const double x = one_center_value(sA, a < l ? a : l, a < l ? l : a, b < s ? b : s, b < s ? s : b);
-      if (x != 0.0) K += m.P[pk(fA + l, fA + s)] * x;
-    }
-  const int i = fA + b, j = fA + a;  // i >= j
-  const int64_t ij = tri(i) + j;
+  double Pa[16];
+#pragma unroll
+  for (int l = 0; l < 4; ++l)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) Pa[4 * l + s] = (l < nA && s < nA) ? m.P[pk(fA + l, fA + s)] : 0.0;
   double Jv = J[wq_offset(m, A) + pq];
   if (sA != 0) {  // heavy-heavy partial sums: rows b <= a, then columns b > a
     const int a_ = m.hb[A];
-    for (int b_ = 0; b_ <= a_; ++b_) Jv += xs[(tri(a_) + b_) * 20 + pq];
-    for (int b_ = a_ + 1; b_ < nh; ++b_) Jv += xs[(tri(b_) + a_) * 20 + 10 + pq];
+    double r0 = 0.0, r1 = 0.0;
+    for (int b_ = 0; b_ <= a_; ++b_) r0 += xs[(tri(a_) + b_) * 20 + pq];
+    for (int b_ = a_ + 1; b_ < nh; ++b_) r1 += xs[(tri(b_) + a_) * 20 + 10 + pq];
+    Jv += r0 + r1;
   }
+  double K = 0.0;
+#pragma unroll
+  for (int l = 0; l < 4; ++l)
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      if (l >= nA || s >= nA) continue;
+      const double x = one_center_value(sA, a < l ? a : l, a < l ? l : a, b < s ? b : s, b < s ? s : b);
+      if (x != 0.0) K += Pa[4 * l + s] * x;
+    }
+  const int i = fA + b, j = fA + a;  // i >= j
+  const int64_t ij = tri(i) + j;
   const double h = m.H[ij], fv = h + (Jv - 0.5 * K);
   m.F[ij] = fv;
   if (Fs) {
