@@ -133,6 +133,7 @@ struct GridWork {
   size_t bytes = 0;
   double *G = nullptr, *Fprev = nullptr, *wq = nullptr, *dval = nullptr, *partial = nullptr;
   double* X2 = nullptr;  // purification product (G holds X)
+  unsigned* count = nullptr;  // last-block counter of the fused reductions (0 between uses)
   // DIIS history (grid path, when enabled): depth x (F, error) n x n pairs, and the B matrix
   double* diis = nullptr;
   int diis_cap = 0;
@@ -568,6 +569,7 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
                owq = take(8 * (3 * n + 8)), odv = take(8 * n), opart = take(8 * 2 * kPartialMax),
                osc = take(8 * 16),
                oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
+               ocount = take(8),
                owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
   if (ctx->budget && ctx->in_use + off > ctx->budget)
     return fail(ctx, SGB_E_NOMEM, "grid workspace needs %zu bytes over the budget", off);
@@ -582,6 +584,8 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
   w.occ = (int*)(b + oocc); w.vir = (int*)(b + ovir); w.flag = (int*)(b + oflag);
   w.result = (int*)(b + ores); w.worst = (unsigned long long*)(b + owst);
   w.bar = (unsigned*)(b + obar); w.err = (int*)(b + oerr);
+  w.count = (unsigned*)(b + ocount);
+  CUDA_TRY(ctx, cudaMemsetAsync(w.count, 0, 8, ctx->stream));
   return SGB_OK;
 }
 
@@ -715,14 +719,17 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
   float* Y32 = X32 + nn;
   bool fp32 = mixed;
+  bool fused = !fp32;  // the FP64 kernels finish their sums themselves
   if (fp32)
     k_pur_init32<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X32, w.partial);
   else
-    k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial);
+    k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial, w.count, sc + 4);
   double t[2];
   auto sums = [&]() -> int {
-    k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
-    k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nb, nb, sc + 5);
+    if (!fused) {
+      k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
+      k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nb, nb, sc + 5);
+    }
     CUDA_TRY(ctx, cudaGetLastError());
     CUDA_TRY(ctx, cudaMemcpyAsync(t, sc + 4, 16, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
@@ -740,6 +747,7 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
       k_pur_widen<<<nb, kGridThreads, 0, st>>>(nn, X32, X, n, w.partial);
       if ((rc = sums())) return rc;
       fp32 = false;
+      fused = true;
     }
     if (tail < 0 && t[0] - t[1] < kPurifyIdem) tail = kPurifyTail;
     if (tail == 0) {
@@ -762,7 +770,7 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
       if (cublasDsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &one, X, n, &zero,
                       w.X2, n) != CUBLAS_STATUS_SUCCESS)
         return fail(ctx, SGB_E_CUDA, "cublasDsyrk failed (n = %d)", n);
-      k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial);
+      k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial, w.count, sc + 4);
     }
     if ((rc = sums())) return rc;
   }

@@ -158,6 +158,45 @@ __global__ void k_reduce_sum(const double* partial, int n, double* out) {
 // triangle, column-major); these kernels build X_0, apply the chosen branch and reduce tr X and
 // ||X||_F^2 -- block partials, then one fixed-order pass, so the sums are deterministic.
 
+// Block partials of (a, b); the last block to finish adds them up in a fixed order into
+// out[0..1] (so the totals do not depend on which block is last) and resets *count, which must
+// be 0 on entry.  Saves the second-pass launches between the products.
+__device__ void finalize_sums2(double a, double b, double* partial, unsigned* count,
+                               double* out) {
+  write_block_partial(a, partial);
+  __syncthreads();
+  write_block_partial(b, partial + gridDim.x);
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(count, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s1 = 0.0, s2 = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+    s1 += __ldcg(partial + i);
+    s2 += __ldcg(partial + gridDim.x + i);
+  }
+  __shared__ double r1[32], r2[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+  }
+  if ((threadIdx.x & 31) == 0) { r1[threadIdx.x >> 5] = s1; r2[threadIdx.x >> 5] = s2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t1 = 0.0, t2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { t1 += r1[w]; t2 += r2[w]; }
+    out[0] = t1;
+    out[1] = t2;
+    *count = 0;
+  }
+}
+
 // Gershgorin bounds: per block, min over its rows of F_ii - r_i and max of F_ii + r_i
 // (partial[2 blk], partial[2 blk + 1]); warp per row.
 __global__ void k_pur_bounds(int n, const double* __restrict__ F, double* partial) {
@@ -195,7 +234,7 @@ __global__ void k_pur_bounds_reduce(const double* partial, int nb, double* lohi)
 // X_0 = (hi I - F) / (hi - lo); block partials of tr X (partial[blk]) and ||X||^2
 // (partial[gridDim + blk]).
 __global__ void k_pur_init(int n, const double* __restrict__ F, const double* lohi, double* X,
-                           double* partial) {
+                           double* partial, unsigned* count, double* out) {
   const double lo = lohi[0], hi = lohi[1], inv = 1.0 / (hi - lo);
   const int64_t nn = (int64_t)n * n;
   double s1 = 0.0, s2 = 0.0;
@@ -206,15 +245,13 @@ __global__ void k_pur_init(int n, const double* __restrict__ F, const double* lo
     if (i == j) s1 += v;
     s2 = fma(v, v, s2);
   }
-  write_block_partial(s1, partial);
-  __syncthreads();
-  write_block_partial(s2, partial + gridDim.x);
+  finalize_sums2(s1, s2, partial, count, out);
 }
 
 // X <- X2 (sq) or 2X - X2 on the lower triangle of X2 (column-major), mirrored; partial sums
 // of the new tr X and ||X||^2 as in k_pur_init.
 __global__ void k_pur_update(int n, double* X, const double* __restrict__ X2, int sq,
-                             double* partial) {
+                             double* partial, unsigned* count, double* out) {
   const int64_t nn = (int64_t)n * n;
   double s1 = 0.0, s2 = 0.0;
   for (int64_t t = gtid(); t < nn; t += gstride()) {
@@ -227,9 +264,7 @@ __global__ void k_pur_update(int n, double* X, const double* __restrict__ X2, in
     if (i == j) s1 += v;
     s2 = fma(i == j ? v : 2.0 * v, v, s2);
   }
-  write_block_partial(s1, partial);
-  __syncthreads();
-  write_block_partial(s2, partial + gridDim.x);
+  finalize_sums2(s1, s2, partial, count, out);
 }
 
 // Mixed precision: the same two kernels on an FP32 X (products on the tensor cores as
