@@ -62,17 +62,17 @@ int sgb_ctx_synchronize(sgb_ctx *ctx);
 const char *sgb_last_error(const sgb_ctx *ctx);
 const char *sgb_status_string(int status);
 /* How an SCF step gets the density P from F (no counterpart in the reference, which always
- * diagonalises with LAPACK dsyev, scfcalculation.cpp:94-110):
- *   SGB_SOLVER_PURIFY (default) -- trace-correcting purification on the FP64 tensor-core path
- *     for nao <= 160 (the same aufbau projector; a Jacobi eigensolve replaces it for a step
- *     where it does not converge, and gives the eigenpairs at the end of sgb_scf);
+ *   diagonalises with LAPACK dsyev, scfcalculation.cpp:94-110):
+ *   SGB_SOLVER_PURIFY (default) -- trace-correcting purification on the FP64 tensor cores (the
+ *     same aufbau projector; a Jacobi eigensolve replaces it for a step where it does not
+ *     converge, and gives the eigenpairs when they are asked for);
  *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step;
  *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: for one large molecule (the grid path,
  *     nao > 160) the purification products run in FP32 until the recursion is near idempotent
  *     and finish in FP64 (Fock, energies and the convergence test stay FP64); the one-CTA path
  *     keeps FP64 products.
- * Molecules above nao 160 always diagonalise.  The environment variable
- * SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for sgb_scf_noalloc). */
+ * The environment variable SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for
+ * sgb_scf_noalloc). */
 #define SGB_SOLVER_PURIFY 0
 #define SGB_SOLVER_JACOBI 1
 #define SGB_SOLVER_PURIFY_MIXED 2
@@ -136,9 +136,9 @@ int sgb_heat_of_formation(int natoms, const int *Z, double e_tot, double *dhf_kc
 int sgb_mol_create(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, sgb_mol **out);
 int sgb_mol_destroy(sgb_mol *mol);
 /* Execution path of the stage calls: AUTO picks one CTA per molecule with its SCF matrices in
- * shared memory for nao <= 160 and the grid-wide kernels (host-driven SCF loop, cooperative
- * Jacobi) above that; CTA / GRID force one (CTA streams its eigensolver matrices from global
- * memory above nao 160 and refuses SCF above nao 1024). */
+ * shared memory for nao <= 160 and the grid-wide kernels (host-driven SCF loop, products on the
+ * whole GPU) above that; CTA / GRID force one (CTA keeps its work matrices in global memory
+ * above nao 160 and refuses SCF above nao 1024). */
 #define SGB_PATH_AUTO 0
 #define SGB_PATH_CTA 1
 #define SGB_PATH_GRID 2

@@ -3,10 +3,11 @@
 // Molecules are handed out in the order given by `order` (the host sorts by estimated cost,
 // largest first, so the tail of the launch holds the cheap ones).
 //
-// Shared memory holds the eigensolver's working matrix G = F V (odd leading
-// dimension) and, for nao <= 110, the eigenvectors V as well; the per-atom pair densities and a
-// few reduction slots follow.  Hcore, P, F (packed and full) live in global memory
-// (L2-resident at these sizes), as does V for the larger molecules.
+// Shared memory holds the matrix the density step works on (purification's X, or the Jacobi
+// working matrix G = F V and, for nao <= 110, the eigenvectors V), which the Fock build reuses
+// as staging space; the per-atom pair densities, Coulomb sums and a few reduction slots follow.
+// Hcore, P, F (packed and full) live in global memory (L2-resident at these sizes), as do V and,
+// above nao 160, the work matrices.
 //
 // The SCF loop is the reference's (scfcalculation.cpp:66-146): guess P -> F -> E_0, then
 // repeat {eigensolve F -> P from the nocc lowest vectors -> F -> E} until |dE| < tol or
@@ -43,7 +44,7 @@ struct BatchArgs {
   double* V;
   double* T;
   double* eig;
-  double* W;        // eigensolver work matrices of the molecules above nao 160
+  double* W;        // work matrices (X and its partner, or G) of the molecules above nao 160
   double* e_el;
   double* e_cc;
   int* n_iter;
@@ -128,7 +129,8 @@ constexpr double kCrossMargin = 1.0;
 // would start below n * 3e-6^2 / 1 eV ~ 1e-9 eV (n <= 160), so no confirmation sweep is run.
 constexpr double kJacobiDoneGapped = 3e-6;
 
-// Largest nao whose G fits one CTA's shared memory; above it G and V are global (streamed).
+// Largest nao whose work matrix fits one CTA's shared memory; above it the work matrices (and
+// V) are in global memory.
 constexpr int kGsmemMax = 160;
 
 // The Fock build keeps its staging buffers and heavy-heavy partial sums in the matrix region
