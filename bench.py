@@ -252,6 +252,13 @@ def run_ours(args):
     nb = args.batch
     mols = geo.batch_c3(nb, seed=rank)
     ctx = sg.Context(local)
+    tuned = None
+    if not args.no_tune:
+        # CTA size per nao size class, chosen by timing this batch (semigpu_b200/autotune.py);
+        # untimed, before the warm-up
+        from semigpu_b200 import autotune
+
+        tuned = autotune.tune(ctx, mols, repeats=2)
     batch = sg.Batch(ctx, mols)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2
 
@@ -392,6 +399,9 @@ def run_ours(args):
             "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "molecules_per_gpu": nb, "tol_eV": TOL,
+                       "class_threads": tuned["class_threads"] if tuned else
+                       [t for _, t in sg.size_classes()],
+                       "autotuned": tuned is not None,
                        "precision": "fp64", "parallelism": f"replicas x{world}",
                        "l2": "working set > L2 (integrals + eigenvector arenas); a 256 MB "
                              "buffer is written between timed steps"},
@@ -429,6 +439,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=BATCH,
                     help="molecules per GPU (default: the 4096-molecule workload)")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="keep the default CTA size per size class (skip the autotuner)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="device-timed launches only (no e2e, plain-path or CPU legs); used "
                          "for profiler captures of a smaller batch")

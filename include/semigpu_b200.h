@@ -77,6 +77,13 @@ const char *sgb_status_string(int status);
 #define SGB_SOLVER_JACOBI 1
 #define SGB_SOLVER_PURIFY_MIXED 2
 int sgb_ctx_set_density_solver(sgb_ctx *ctx, int solver);
+/* The size classes of the batched launch (no counterpart in the reference): *count classes,
+ * class k takes molecules up to nao_max[k] AOs and launches CTAs of threads[k] threads by
+ * default (arrays of max_count entries; either may be NULL).  sgb_ctx_set_class_threads sets
+ * the CTA size per class for this context (128 only for the classes up to nao 64, 512 for the
+ * large-molecule class); semigpu_b200/autotune.py picks them by timing. */
+int sgb_size_classes(int *count, int *nao_max, int *threads, int max_count);
+int sgb_ctx_set_class_threads(sgb_ctx *ctx, int count, const int *threads);
 /* Caps the batched launches of this context at share x (number of SMs) CTAs' worth of SMs
  * (0 < share <= 1; 1 = the whole GPU, the default).  No counterpart in the reference; a
  * server running several contexts side by side uses it so that one context's persistent

@@ -43,6 +43,8 @@ SIGNATURES = {
     "sgb_ctx_set_density_solver": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_ctx_set_sm_share": (ctypes.c_int, [_VP, ctypes.c_double]),
     "sgb_ctx_set_diis": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sgb_size_classes": (ctypes.c_int, [_I, _I, _I, ctypes.c_int]),
+    "sgb_ctx_set_class_threads": (ctypes.c_int, [_VP, ctypes.c_int, _I]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
     "sgb_heat_of_formation": (ctypes.c_int, [ctypes.c_int, _I, ctypes.c_double, _D]),
     "sgb_mol_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.POINTER(_VP)]),
@@ -114,6 +116,16 @@ def heat_of_formation(Z, e_tot: float) -> float:
     return out.value
 
 
+def size_classes() -> list[tuple[int, int]]:
+    """(largest nao, default CTA threads) of each size class of the batched launch."""
+    cnt = ctypes.c_int()
+    lib().sgb_size_classes(ctypes.byref(cnt), None, None, 0)
+    nmax = np.zeros(cnt.value, np.int32)
+    thr = np.zeros(cnt.value, np.int32)
+    lib().sgb_size_classes(ctypes.byref(cnt), _i(nmax), _i(thr), cnt.value)
+    return [(int(a), int(b)) for a, b in zip(nmax, thr)]
+
+
 def mndo_parameters(z: int) -> np.ndarray:
     """The engine's MNDO parameters of element z (order of the SGB_P_* indices)."""
     out = np.zeros(18)
@@ -151,6 +163,11 @@ class Context:
         """SOLVER_PURIFY (default), SOLVER_JACOBI or SOLVER_PURIFY_MIXED for the SCF steps of
         later calls."""
         self.check(lib().sgb_ctx_set_density_solver(self.h, int(solver)), "set_density_solver")
+
+    def set_class_threads(self, threads):
+        """CTA size per size class for this context's batched launches (see size_classes)."""
+        t = np.ascontiguousarray(threads, np.int32)
+        self.check(lib().sgb_ctx_set_class_threads(self.h, len(t), _i(t)), "set_class_threads")
 
     def set_diis(self, depth: int):
         """Pulay DIIS of this depth (0 = off) for single-molecule runs on the grid path."""

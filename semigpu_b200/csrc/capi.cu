@@ -47,6 +47,14 @@ int default_solver() {
   return SOLVER_PURIFY;
 }
 
+// CTA sizes a class can launch with (launch_class): the streamed class only 512 threads, the
+// classes whose columns fit 2 registers per lane also 128.
+bool class_threads_ok(int k, int t) {
+  if (k < 0 || k >= kNumClasses) return false;
+  if (kClasses[k].cr == 0) return t == 512;
+  return t == 256 || t == 512 || (t == 128 && kClasses[k].cr == 2);
+}
+
 int class_of(int nao) {
   int c = 0;
   while (nao > kClasses[c].nmax) ++c;
@@ -1121,11 +1129,11 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
     }
   }
   c->solver = default_solver();
-  if (const char* env = getenv("SGB_CLASS_THREADS")) {  // e.g. "256,512,512,512"
+  if (const char* env = getenv("SGB_CLASS_THREADS")) {  // e.g. "128,256,512,512,512"
     int k = 0;
     for (const char* p = env; *p && k < kNumClasses; ++k) {
       const int t = atoi(p);
-      if (t == 256 || t == 512 || (t == 128 && kClasses[k].cr == 2)) c->class_threads[k] = t;
+      if (class_threads_ok(k, t)) c->class_threads[k] = t;
       while (*p && *p != ',') ++p;
       if (*p == ',') ++p;
     }
@@ -1142,6 +1150,25 @@ int sgb_ctx_set_density_solver(sgb_ctx* ctx, int solver) {
   ctx->solver = solver == SGB_SOLVER_JACOBI         ? SOLVER_JACOBI
                 : solver == SGB_SOLVER_PURIFY_MIXED ? SOLVER_PURIFY_MIXED
                                                     : SOLVER_PURIFY;
+  return SGB_OK;
+}
+
+int sgb_size_classes(int* count, int* nao_max, int* threads, int max_count) {
+  if (!count) return SGB_E_ARG;
+  *count = kNumClasses;
+  for (int k = 0; k < kNumClasses && k < max_count; ++k) {
+    if (nao_max) nao_max[k] = kClasses[k].nmax;
+    if (threads) threads[k] = kClasses[k].threads;
+  }
+  return SGB_OK;
+}
+
+int sgb_ctx_set_class_threads(sgb_ctx* ctx, int count, const int* threads) {
+  if (!ctx || !threads || count < 0 || count > kNumClasses) return SGB_E_ARG;
+  for (int k = 0; k < count; ++k)
+    if (!class_threads_ok(k, threads[k]))
+      return fail(ctx, SGB_E_ARG, "size class %d cannot run %d-thread CTAs", k, threads[k]);
+  for (int k = 0; k < count; ++k) ctx->class_threads[k] = threads[k];
   return SGB_OK;
 }
 

@@ -42,3 +42,14 @@ def test_status_strings_without_gpu():
     L = sg.lib()
     assert L.sgb_status_string(0) == b"ok"
     assert L.sgb_status_string(-2).startswith(b"element")
+
+
+def test_size_classes_cover_the_batched_range():
+    """The batched launch's size classes: increasing nao bounds up to the single-CTA limit of
+    1024 (then the grid-path class), default CTA sizes 128/256/512."""
+    import semigpu_b200 as sg
+
+    cls = sg.size_classes()
+    bounds = [n for n, _ in cls]
+    assert bounds == sorted(bounds) and bounds[0] == 32 and 1024 in bounds
+    assert {t for _, t in cls} <= {128, 256, 512}
