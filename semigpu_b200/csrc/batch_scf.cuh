@@ -99,9 +99,9 @@ enum : int { STAGE_INTS = 1, STAGE_HCORE = 2, STAGE_SCF = 4, STAGE_CC = 8, STAGE
 
 enum : int { MOL_OK = 0, MOL_EIG_FAILED = 1, MOL_NAN = 2 };
 
-// SOLVER_PURIFY_MIXED: as SOLVER_PURIFY, with the products of the grid path (one large
-// molecule) in FP32 until the recursion is near idempotent, FP64 after; the one-CTA path keeps
-// FP64 products.
+// SOLVER_PURIFY_MIXED: as SOLVER_PURIFY, with the products in FP32 until the recursion is near
+// idempotent, FP64 after: on the tensor cores (tcgen05 kind::tf32, split in two TF32 parts) for
+// one-CTA molecules of nao 65-128, as FP32 SSYRK on the grid path; other sizes keep FP64.
 enum : int { SOLVER_PURIFY = 0, SOLVER_JACOBI = 1, SOLVER_PURIFY_MIXED = 2 };
 
 __host__ __device__ inline int smem_ld(int n) { return n | 1; }
@@ -292,13 +292,18 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {
         // ---- P from F by purification; a Jacobi eigensolve if that fails ----
-        int prod;
+        int prod = -1;
         const double* Xr = smem;
         if constexpr (PLACE == 2) {  // X and its partner in the global work matrix
           double* Xo = nullptr;
           prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq, red,
                                          &Xo);
           Xr = Xo;
+        } else if (NT == 512 && a.solver == SOLVER_PURIFY_MIXED && purify_n16(n) > 64 &&
+                   purify_n16(n) <= 128 && (size_t)128 * purify_n16(n) <= a.mat_doubles) {
+          // mixed form: TF32 tensor-core products (tcgen05), FP64 finish; X's region holds the
+          // 128-row split copies (2 x 128 x n16 floats)
+          if constexpr (NT == 512) prod = block_purify_mixed<NT>(Ffull, n, m.nocc, smem, wq, red);
         } else {
           prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
         }

@@ -362,14 +362,12 @@ __device__ __noinline__ void purify_step(double* X, int n16, int ld, bool sq, do
 // Purifies F (row-major n x n in global memory) into X = P / 2 in shared memory.  Returns the
 // number of products, or -1 (no convergence, wrong trace or a non-finite value).  lz: 3 n
 // doubles of shared scratch; red: 64 doubles.
+// The recursion from the current X (trace t1, squared norm t2) on, products numbered from it0.
 template <int NT>
-__device__ int block_purify(const double* F, int n, int nocc, double* X, double* lz,
-                            double* red) {
-  const int ld = purify_ld(n), n16 = purify_n16(n);
-  double t1, t2;
-  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+__device__ int purify_fp64_loop(double* X, int n16, int ld, int nocc, double* red, double t1,
+                                double t2, int it0) {
   int tail = -1;
-  for (int it = 0; it <= kPurifyMaxIter; ++it) {
+  for (int it = it0; it <= kPurifyMaxIter; ++it) {
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) return -1;
     if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
     if (tail == 0) return fabs(t1 - (double)nocc) < kPurifyTraceTol ? it : -1;
@@ -393,6 +391,252 @@ __device__ int block_purify(const double* F, int n, int nocc, double* X, double*
       return -1;  // 128-thread CTAs only take nao <= 64 (at most 10 super-tiles)
   }
   return -1;
+}
+
+template <int NT>
+__device__ int block_purify(const double* F, int n, int nocc, double* X, double* lz,
+                            double* red) {
+  const int ld = purify_ld(n), n16 = purify_n16(n);
+  double t1, t2;
+  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, t1, t2, 0);
+}
+
+// ------------------------------------------------------------------------------------------
+// Mixed precision on the 5th-generation tensor cores (SOLVER_PURIFY_MIXED, 64 < n16 <= 128):
+// the products of the recursion run as tcgen05.mma kind::tf32 with the accumulator in tensor
+// memory, X split into two TF32 parts (hi = X with the low 13 mantissa bits cleared, lo = X - hi)
+// and X^2 ~ hi hi + hi lo + lo hi (FP32-level accuracy, "3xTF32").  hi and lo sit in shared
+// memory in the K-major no-swizzle canonical layout of the MMA (8-row x 16-byte core matrices:
+// element (r, k) at float ((r/8)(n16/4) + k/4) 32 + (r%8) 4 + k%4, 128 rows, rows past n16
+// zero), so one descriptor pair serves as A (M = 128) and, X being symmetric, as B (N = n16).
+// One thread issues the 3 n16 / 8 MMAs of a product and commits them to an mbarrier; every warp
+// then reads its 32 rows x 32 columns of X^2 from tensor memory (tcgen05.ld 32x32b), forms the
+// branch, re-splits and writes back.  When tr(X - X^2) < kPurifyMixedSwitch, X is symmetrised
+// into FP64 and the recursion finishes with FP64 products (purify_fp64_loop), so the result has
+// FP64 idempotency and the FP32 phase perturbs the occupied subspace only at the 1e-6 level.
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ int kmajor_index(int r, int k, int K) {
+  return ((r >> 3) * (K >> 2) + (k >> 2)) * 32 + (r & 7) * 4 + (k & 3);
+}
+// Shared-memory matrix descriptor: start address, leading (K-direction) and stride
+// (8-row-group) byte offsets, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t umma_smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | ((uint64_t)1 << 46);
+}
+// Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major, M x N.
+__device__ __forceinline__ uint32_t umma_idesc_tf32(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+constexpr int kMbarSpins = 1 << 22;  // bounded wait for the MMAs (a few hundred ms at most)
+// FP32 products until tr(X - X^2) falls below this (3xTF32 keeps X to ~1e-7, so the
+// idempotency error is still well above its FP32 floor of ~1e-5 here)
+constexpr double kPurifyTensorSwitch = 1e-4;
+
+// Splits v into its TF32 head and the FP32 remainder at canonical position idx.
+__device__ __forceinline__ void put_split(float* hi, float* lo, int idx, float v) {
+  const float h = __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
+  hi[idx] = h;
+  lo[idx] = v - h;
+}
+
+template <int NT>
+__device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc, double* X,
+                                               double* lz, double* red) {
+  constexpr int NW = NT / 32;
+  static_assert(NT == 512, "the tensor-memory epilogue maps 16 warps onto 4 x 4 tiles of 32");
+  const int ld = purify_ld(n), n16 = purify_n16(n);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double t1, t2;
+  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+  // ---- X (FP64, row stride ld) -> hi / lo (FP32 canonical, 128 rows) through registers ----
+  float* hi = reinterpret_cast<float*>(X);
+  float* lo = hi + 128 * n16;
+  constexpr int kPer = 128 * 128 / NT;  // elements per thread (n16 <= 128)
+  float keep[kPer];
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int t = threadIdx.x + e * NT, r = t / 128, c = t % 128;
+    keep[e] = (r < n16 && c < n16) ? (float)X[r * ld + c] : 0.0f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int t = threadIdx.x + e * NT, r = t / 128, c = t % 128;
+    if (c < n16) put_split(hi, lo, kmajor_index(r, c, n16), keep[e]);
+  }
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(lz);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(lz + 1);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  if (warp == 0)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(128));
+  asm volatile("fence.proxy.async.shared::cta;");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_tf32(128, n16);
+  const uint32_t lbo = 128, sbo = (uint32_t)(n16 / 4) * 128;
+  const int row = 32 * (warp & 3) + lane, c0 = (warp >> 2) * 32;
+  const uint32_t taddr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)c0;
+  // the 32 elements (row, c0 .. c0 + 31) this thread rewrites after every product stay in
+  // registers, so the epilogue reads only tensor memory
+  float xr[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int c = c0 + j;
+    xr[j] = 0.0f;
+    if (row < n16 && c < n16) {
+      const int idx = kmajor_index(row, c, n16);
+      xr[j] = hi[idx] + lo[idx];
+    }
+  }
+  int it = 0, status = 0;
+  uint32_t phase = 0;
+  for (; it < kPurifyMaxIter; ++it) {
+    if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) { status = -1; break; }
+    if (fabs(t1 - t2) < kPurifyTensorSwitch) break;
+    const double n_o = (double)nocc;
+    const bool sq = fabs(t2 - n_o) < fabs(2.0 * t1 - t2 - n_o);
+    if (threadIdx.x == 0) {
+      int first = 1;
+      for (int k0 = 0; k0 < n16; k0 += 8) {
+        const uint32_t off = (uint32_t)(k0 / 4) * 128;
+        const uint64_t dh = umma_smem_desc(smem_u32(hi) + off, lbo, sbo);
+        const uint64_t dl = umma_smem_desc(smem_u32(lo) + off, lbo, sbo);
+        const uint64_t da[3] = {dh, dh, dl}, db[3] = {dh, dl, dh};
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                       "l"(da[q]), "l"(db[q]), "r"(idesc), "r"(first ? 0 : 1));
+          first = 0;
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(mbar)));
+    }
+    uint32_t done = 0;
+    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n\t}"
+                   : "=r"(done)
+                   : "r"(smem_u32(mbar)), "r"(phase));
+      if (!done) __nanosleep(64);
+    }
+    // every thread takes the same branch: the MMAs completed for all or the step is abandoned
+    if (__syncthreads_or(!done)) {
+      status = -2;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    uint32_t v[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+        "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;");
+    double s1 = 0.0, s2 = 0.0;
+    if (row < n16) {
+#pragma unroll
+      for (int g = 0; g < 8; ++g) {  // four columns = 16 contiguous bytes of a core matrix row
+        const int c = c0 + 4 * g;
+        if (c < n16) {
+          float h4[4], l4[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int j = 4 * g + q;
+            const float d = __uint_as_float(v[j]);
+            const float nv = sq ? d : fmaf(2.0f, xr[j], -d);
+            xr[j] = nv;
+            h4[q] = __uint_as_float(__float_as_uint(nv) & 0xFFFFE000u);
+            l4[q] = nv - h4[q];
+            if (row == c + q) s1 += nv;
+            s2 = fma((double)nv, (double)nv, s2);
+          }
+          const int idx = kmajor_index(row, c, n16);
+          *reinterpret_cast<float4*>(hi + idx) = make_float4(h4[0], h4[1], h4[2], h4[3]);
+          *reinterpret_cast<float4*>(lo + idx) = make_float4(l4[0], l4[1], l4[2], l4[3]);
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    double* part = red + 32 * (it & 1);
+    if (lane == 0) { part[warp] = s1; part[16 + warp] = s2; }
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();  // X rewritten, tensor memory read: the next product may start
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    s1 = 0.0;
+    s2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) { s1 += part[k]; s2 += part[16 + k]; }
+    t1 = s1;
+    t2 = s2;
+  }
+  if (status == -2) {
+    // MMAs still outstanding after the bounded wait: wait once more (bounded) before giving the
+    // tensor memory back; the step is then diagonalised instead
+    uint32_t done = 0;
+    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n\t}"
+                   : "=r"(done)
+                   : "r"(smem_u32(mbar)), "r"(phase));
+      if (!done) __nanosleep(64);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(mbar)));
+  if (status < 0) return -1;
+  if (it == kPurifyMaxIter) return -1;
+  // ---- back to FP64, symmetrised (the tensor-core products are not bit-symmetric) ----
+  double back[kPer];
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int t = threadIdx.x + e * NT, r = t / 128, c = t % 128;
+    back[e] = 0.0;
+    if (r < n16 && c < n16) {
+      const int a = kmajor_index(r, c, n16), b = kmajor_index(c, r, n16);
+      back[e] = 0.5 * (((double)hi[a] + (double)lo[a]) + ((double)hi[b] + (double)lo[b]));
+    }
+  }
+  __syncthreads();
+  double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int t = threadIdx.x + e * NT, r = t / 128, c = t % 128;
+    if (r < n16 && c < n16) {
+      X[r * ld + c] = back[e];
+      if (r == c) s1 += back[e];
+      s2 = fma(back[e], back[e], s2);
+    }
+  }
+  for (int t = threadIdx.x; t < n16 * 4; t += NT) X[(t >> 2) * ld + n16 + (t & 3)] = 0.0;  // pad
+  block_sum2<NT>(s1, s2, red);
+  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it);
 }
 
 // Above nao 160 X does not fit in shared memory: X and Y (n16 x n16, row stride n16 + 4) live

@@ -132,3 +132,27 @@ def test_diis_converges_to_the_same_energy_in_no_more_steps():
     assert plain["converged"] and diis["converged"]
     assert diis["n_iter"] <= plain["n_iter"]
     assert abs(diis["E_tot"] - plain["E_tot"]) < 1e-5
+
+
+def test_mixed_tensor_core_products_in_batch(gpu_ctx):
+    """Mixed form in the batch: nao 65-128 purify with TF32 tcgen05 products (3xTF32) and an FP64
+    finish; every molecule converges within 1e-4 eV of the FP64 form, without a fallback."""
+    rng = np.random.default_rng(17)
+    mols = [geo.alkane(k, rng) for k in (11, 13, 15, 17, 19, 21)]  # nao 68 .. 128
+    mols += [geo.polyene(k, rng) for k in (14, 18, 22, 24)]           # nao 72 .. 122
+    assert all(64 < m.nao <= 128 for m in mols)
+    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ctx = sg.Context(0)
+    try:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        b = sg.Batch(ctx, mols)
+        b.set_profiling(True)
+        b.run(1e-6)
+        r = b.results()
+        sc = b.stage_cycles()
+        b.close()
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
+    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
