@@ -69,8 +69,9 @@ const char *sgb_status_string(int status);
  *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step;
  *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: for one large molecule (the grid path,
  *     nao > 160) the purification products run in FP32 until the recursion is near idempotent
- *     and finish in FP64 (Fock, energies and the convergence test stay FP64); the one-CTA path
- *     keeps FP64 products.
+ *     and finish in FP64 (Fock, energies and the convergence test stay FP64); in a batch,
+ *     molecules of 65-128 AOs run the FP32-level products on the tcgen05 tensor cores (TF32,
+ *     split in two parts) before the FP64 finish, other sizes keep FP64 products.
  * The environment variable SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for
  * sgb_scf_noalloc). */
 #define SGB_SOLVER_PURIFY 0
@@ -101,7 +102,9 @@ int sgb_ctx_set_diis(sgb_ctx *ctx, int depth);
  * synchronises the whole device, which would stall other contexts' work).  One batch at a time
  * uses the arena; bytes = 0 releases it. */
 int sgb_ctx_reserve(sgb_ctx *ctx, size_t bytes);
-/* Bytes of device memory currently held by the context's molecules and batches. */
+/* Bytes of device memory currently held by the context: its molecules and batches, and the
+ * arenas of destroyed ones that it keeps for reuse (at most 16 of them and 8 GiB; released
+ * when the budget or a failed allocation needs the room, and by sgb_ctx_destroy). */
 size_t sgb_ctx_bytes_in_use(const sgb_ctx *ctx);
 
 /* ---- MNDO element data ------------------------------------------------------------------ */

@@ -97,6 +97,14 @@ struct sgb_ctx {
   char* pool = nullptr;
   size_t pool_bytes = 0;
   bool pool_busy = false;
+  // Device arenas given back by destroyed batches, molecules and grid workspaces, kept for the
+  // next ones: cudaFree synchronises the whole device and cudaMalloc can wait behind running
+  // kernels, so create/destroy cycles of similar sizes (one molecule per call) allocate
+  // nothing once warm.  Counted in in_use; released when the budget or a failed cudaMalloc
+  // needs the room, and with the context.
+  std::vector<std::pair<char*, size_t>> spare;
+  size_t spare_bytes = 0;
+  std::mutex spare_mutex;
 };
 
 struct sgb_batch {
@@ -213,13 +221,94 @@ void give_event(sgb_ctx* ctx, cudaEvent_t ev) {
   ctx->events.push_back(ev);
 }
 
+constexpr size_t kSpareMaxBlocks = 16;
+constexpr size_t kSpareMaxBytes = size_t(8) << 30;
+
+// Arena sizes: at least 1 MiB, then four sizes per power of two (at most 25 % over the
+// request), so the arenas of molecules of similar size are interchangeable.
+size_t arena_size_class(size_t bytes) {
+  if (bytes <= (size_t(1) << 20)) return size_t(1) << 20;
+  const int lg = 63 - __builtin_clzll((unsigned long long)bytes);
+  const size_t step = size_t(1) << (lg - 2);
+  return (bytes + step - 1) / step * step;
+}
+
+// Frees spare arenas, largest first, until at most keep_blocks / keep_bytes remain and
+// in_use + need fits the budget.  Caller holds spare_mutex.
+void release_spares(sgb_ctx* ctx, size_t keep_blocks, size_t keep_bytes, size_t need = 0) {
+  while (!ctx->spare.empty() &&
+         (ctx->spare.size() > keep_blocks || ctx->spare_bytes > keep_bytes ||
+          (ctx->budget && ctx->in_use + need > ctx->budget))) {
+    auto big = std::max_element(ctx->spare.begin(), ctx->spare.end(),
+                                [](const std::pair<char*, size_t>& a,
+                                   const std::pair<char*, size_t>& b) { return a.second < b.second; });
+    cudaFree(big->first);
+    ctx->spare_bytes -= big->second;
+    ctx->in_use -= big->second;
+    ctx->spare.erase(big);
+  }
+}
+
+// A device arena of at least `bytes`: the best-fitting spare (at most 4x the request), else a
+// new cudaMalloc within the budget.  *got = the arena's size (what arena_put takes back).
+int arena_get(sgb_ctx* ctx, size_t bytes, const char* what, char** out, size_t* got) {
+  std::lock_guard<std::mutex> lock(ctx->spare_mutex);
+  int best = -1;
+  for (int i = 0; i < (int)ctx->spare.size(); ++i) {
+    const size_t sz = ctx->spare[i].second;
+    if (sz >= bytes && sz <= 4 * bytes + (size_t(1) << 20) &&
+        (best < 0 || sz < ctx->spare[best].second))
+      best = i;
+  }
+  if (best >= 0) {
+    *out = ctx->spare[best].first;
+    *got = ctx->spare[best].second;
+    ctx->spare_bytes -= *got;
+    ctx->spare.erase(ctx->spare.begin() + best);
+    return SGB_OK;
+  }
+  const size_t sz = arena_size_class(bytes);
+  release_spares(ctx, kSpareMaxBlocks, kSpareMaxBytes, sz);
+  if (ctx->budget && ctx->in_use + sz > ctx->budget)
+    return fail(ctx, SGB_E_NOMEM, "%s needs %zu bytes; budget %zu, in use %zu", what, sz,
+                ctx->budget, ctx->in_use);
+  cudaError_t e = cudaMalloc(out, sz);
+  if (e != cudaSuccess && !ctx->spare.empty()) {
+    cudaGetLastError();
+    release_spares(ctx, 0, 0);
+    e = cudaMalloc(out, sz);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu) for %s: %s", sz, what, cudaGetErrorString(e));
+  }
+  ctx->in_use += sz;
+  *got = sz;
+  return SGB_OK;
+}
+
+// Takes an arena back once the context's stream (which every launch of the context joins)
+// has finished with it.
+void arena_put(sgb_ctx* ctx, char* p, size_t bytes) {
+  if (!p) return;
+  if (!ctx) {
+    cudaFree(p);
+    return;
+  }
+  cudaStreamSynchronize(ctx->stream);
+  std::lock_guard<std::mutex> lock(ctx->spare_mutex);
+  ctx->spare.emplace_back(p, bytes);
+  ctx->spare_bytes += bytes;
+  release_spares(ctx, kSpareMaxBlocks, kSpareMaxBytes);
+}
+
 void free_batch(sgb_batch* b) {
   if (!b) return;
   if (b->arena && b->from_pool) {
     b->ctx->pool_busy = false;
   } else if (b->arena) {
-    cudaFree(b->arena);
-    if (b->ctx) b->ctx->in_use -= b->bytes;
+    arena_put(b->ctx, b->arena, b->bytes);
   }
   give_event(b->ctx, b->ev0);
   give_event(b->ctx, b->ev1);
@@ -328,17 +417,11 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     b->from_pool = true;
     ctx->pool_busy = true;
   } else {
-    if (ctx->budget && ctx->in_use + off > ctx->budget) {
+    const int rc = arena_get(ctx, off, "batch", &b->arena, &b->bytes);
+    if (rc) {
       delete b;
-      return fail(ctx, SGB_E_NOMEM, "batch needs %zu bytes; budget %zu, in use %zu", off,
-                  ctx->budget, ctx->in_use);
+      return rc;
     }
-    e = cudaMalloc(&b->arena, off);
-    if (e != cudaSuccess) {
-      delete b;
-      return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
-    }
-    ctx->in_use += off;
   }
   char* base = b->arena;
   b->d_desc = (MolDesc*)(base + o_desc);
@@ -579,12 +662,7 @@ int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
                oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
                ocount = take(8),
                owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
-  if (ctx->budget && ctx->in_use + off > ctx->budget)
-    return fail(ctx, SGB_E_NOMEM, "grid workspace needs %zu bytes over the budget", off);
-  cudaError_t e = cudaMalloc(&w.arena, off);
-  if (e != cudaSuccess) return fail(ctx, SGB_E_NOMEM, "cudaMalloc(%zu): %s", off, cudaGetErrorString(e));
-  ctx->in_use += off;
-  w.bytes = off;
+  if (int rc = arena_get(ctx, off, "grid workspace", &w.arena, &w.bytes)) return rc;
   char* b = w.arena;
   w.G = (double*)(b + oG); w.Fprev = (double*)(b + oFp); w.X2 = (double*)(b + oX2);
   w.wq = (double*)(b + owq);
@@ -603,8 +681,7 @@ void free_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
     if (ctx) ctx->in_use -= mol->gw.diis_bytes;
   }
   if (mol->gw.arena) {
-    cudaFree(mol->gw.arena);
-    if (ctx) ctx->in_use -= mol->gw.bytes;
+    arena_put(ctx, mol->gw.arena, mol->gw.bytes);
     mol->gw = GridWork();
   }
 }
@@ -691,7 +768,7 @@ int grid_lanczos_bounds(sgb_ctx* ctx, sgb_mol* mol, double* lohi) {
   if (llo == llo && lhi == lhi) {
     g[0] = std::max(g[0], llo);
     g[1] = std::min(g[1], lhi);
-    CUDA_TRY(ctx, cudaMemcpy(lohi, g, 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(ctx, cudaMemcpyAsync(lohi, g, 16, cudaMemcpyHostToDevice, st));
   }
   return SGB_OK;
 }
@@ -1213,6 +1290,10 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
   free_batch(ctx->cached);
   ctx->cached = nullptr;
   if (ctx->pool) cudaFree(ctx->pool);
+  {
+    std::lock_guard<std::mutex> lock(ctx->spare_mutex);
+    release_spares(ctx, 0, 0);
+  }
   if (ctx->blas) cublasDestroy(ctx->blas);
   for (int k = 0; k < kNumClasses; ++k) {
     if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);

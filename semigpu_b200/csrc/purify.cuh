@@ -412,7 +412,7 @@ __device__ int block_purify(const double* F, int n, int nocc, double* X, double*
 // zero), so one descriptor pair serves as A (M = 128) and, X being symmetric, as B (N = n16).
 // One thread issues the 3 n16 / 8 MMAs of a product and commits them to an mbarrier; every warp
 // then reads its 32 rows x 32 columns of X^2 from tensor memory (tcgen05.ld 32x32b), forms the
-// branch, re-splits and writes back.  When tr(X - X^2) < kPurifyMixedSwitch, X is symmetrised
+// branch, re-splits and writes back.  When tr(X - X^2) < kPurifyTensorSwitch, X is symmetrised
 // into FP64 and the recursion finishes with FP64 products (purify_fp64_loop), so the result has
 // FP64 idempotency and the FP32 phase perturbs the occupied subspace only at the 1e-6 level.
 
