@@ -353,7 +353,7 @@ def run_ours(args):
                  "max_abs_dE_total_eV": float(dE.max()), "tolerance_eV": 1e-4,
                  "n_iter_changed": int(np.sum(rm["n_iter"] != res["n_iter"])),
                  "all_converged": bool(np.all(rm["converged"])),
-                 "form": "TF32 tcgen05 products (3xTF32) for nao 65-128, FP64 elsewhere and "
+                 "form": "TF32 tcgen05 products (3xTF32) for nao 65-160, FP64 elsewhere and "
                          "for the finish of every purification"}
     if rank == 0:
         peak, peak_src = fp64_peak_tflops(torch)

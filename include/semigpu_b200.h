@@ -70,7 +70,7 @@ const char *sgb_status_string(int status);
  *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: for one large molecule (the grid path,
  *     nao > 160) the purification products run in FP32 until the recursion is near idempotent
  *     and finish in FP64 (Fock, energies and the convergence test stay FP64); in a batch,
- *     molecules of 65-128 AOs run the FP32-level products on the tcgen05 tensor cores (TF32,
+ *     molecules of 65-160 AOs run the FP32-level products on the tcgen05 tensor cores (TF32,
  *     split in two parts) before the FP64 finish, other sizes keep FP64 products.
  * The environment variable SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for
  * sgb_scf_noalloc). */

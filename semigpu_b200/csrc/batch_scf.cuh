@@ -243,7 +243,7 @@ __device__ inline void split_by_rank(const double* dval, int n, int nocc, int* o
 // PLACE: 0 = G and V in shared memory (nao <= kVsmemMax), 1 = G in shared memory and V in
 // global memory (nao <= kGsmemMax), 2 = both in global memory (larger; CR must be 0).  A
 // template parameter so every access in the eigensolver has a known address space.
-template <int NT, int CR, int PLACE>
+template <int NT, int CR, int PLACE, int MX>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
   const MolView m = make_view(a, d);
@@ -299,13 +299,17 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
           prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq, red,
                                          &Xo);
           Xr = Xo;
-        } else if (NT == 512 && a.solver == SOLVER_PURIFY_MIXED && purify_n16(n) > 64 &&
-                   purify_n16(n) <= 128 && (size_t)128 * purify_n16(n) <= a.mat_doubles) {
-          // mixed form: TF32 tensor-core products (tcgen05), FP64 finish; X's region holds the
-          // 128-row split copies (2 x 128 x n16 floats)
-          if constexpr (NT == 512) prod = block_purify_mixed<NT>(Ffull, n, m.nocc, smem, wq, red);
         } else {
-          prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
+          bool tensor = false;
+          if constexpr (MX == 1 && NT == 512) {
+            // mixed form: TF32 tensor-core products (tcgen05), FP64 finish; X's region holds
+            // the split copies (2 x max(128, n16) x n16 floats)
+            const int n16 = purify_n16(n);
+            tensor = a.solver == SOLVER_PURIFY_MIXED && n16 > 64 && n16 <= 160 &&
+                     (size_t)(n16 > 128 ? n16 : 128) * n16 <= a.mat_doubles;
+            if (tensor) prod = block_purify_mixed<NT>(Ffull, n, m.nocc, smem, wq, red);
+          }
+          if (!tensor) prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
         }
         clk.lap(ST_PURIFY);
         clk.add(ST_PURIFY_PRODUCTS, (unsigned long long)(prod > 0 ? prod : 0));
@@ -452,7 +456,10 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
 }
 
 // NT threads per CTA; CR column registers per lane in the eigensolver (nao <= 32 * CR).
-template <int NT, int CR>
+// MX = 1: the instance that can take the tensor-core mixed form (launched only for that
+// solver); the FP64 instances carry no call into it, which would change their register
+// allocation.
+template <int NT, int CR, int MX = 0>
 __global__ void __launch_bounds__(NT, 512 / NT) k_batch_scf(BatchArgs a) {
   extern __shared__ double smem[];
   __shared__ int s_next;
@@ -465,12 +472,12 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_batch_scf(BatchArgs a) {
     const int mi = a.order[q];
     const int n = a.mols[mi].nao;
     if constexpr (CR == 0) {
-      run_molecule<NT, 0, 2>(a, mi, smem);
+      run_molecule<NT, 0, 2, MX>(a, mi, smem);
     } else {
       if (n <= kVsmemMax)
-        run_molecule<NT, CR, 0>(a, mi, smem);
+        run_molecule<NT, CR, 0, MX>(a, mi, smem);
       else
-        run_molecule<NT, CR, 1>(a, mi, smem);
+        run_molecule<NT, CR, 1, MX>(a, mi, smem);
     }
   }
 }

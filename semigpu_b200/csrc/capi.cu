@@ -485,9 +485,9 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
 constexpr int kMaxDevices = 64;
 
 // Raises the kernel's cap on the current device (once); *cap receives it.
-template <int NT, int CR>
+template <int NT, int CR, int MX = 0>
 cudaError_t kernel_smem_cap(int* cap) {
-  auto* k = k_batch_scf<NT, CR>;
+  auto* k = k_batch_scf<NT, CR, MX>;
   static int max_dynamic[kMaxDevices] = {};  // 0: not set yet on that device
   static std::mutex set_mutex;
   int dev = 0;
@@ -518,16 +518,18 @@ cudaError_t prepare_kernels() {
       (e = kernel_smem_cap<256, 2>(&c)) || (e = kernel_smem_cap<256, 3>(&c)) ||
       (e = kernel_smem_cap<256, 4>(&c)) || (e = kernel_smem_cap<256, 5>(&c)) ||
       (e = kernel_smem_cap<512, 2>(&c)) || (e = kernel_smem_cap<512, 3>(&c)) ||
-      (e = kernel_smem_cap<512, 4>(&c)) || (e = kernel_smem_cap<512, 5>(&c)))
+      (e = kernel_smem_cap<512, 4>(&c)) || (e = kernel_smem_cap<512, 5>(&c)) ||
+      (e = kernel_smem_cap<512, 3, 1>(&c)) || (e = kernel_smem_cap<512, 4, 1>(&c)) ||
+      (e = kernel_smem_cap<512, 5, 1>(&c)))
     return e;
   return cudaSuccess;
 }
 
-template <int NT, int CR>
+template <int NT, int CR, int MX = 0>
 cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStream_t st) {
-  auto* k = k_batch_scf<NT, CR>;
+  auto* k = k_batch_scf<NT, CR, MX>;
   int cap = 0;
-  cudaError_t e = kernel_smem_cap<NT, CR>(&cap);
+  cudaError_t e = kernel_smem_cap<NT, CR, MX>(&cap);
   if (e != cudaSuccess) return e;
   if (smem > (size_t)cap) return cudaErrorInvalidValue;
   int per_sm = 0;
@@ -543,6 +545,13 @@ cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, s
                          cudaStream_t st) {
   if (cr == 0) return launch_kernel<512, 0>(num_sms, a, smem, st);
   if (threads == 128 && cr == 2) return launch_kernel<128, 2>(num_sms, a, smem, st);
+  if (threads == 512 && a.solver == SOLVER_PURIFY_MIXED && cr >= 3) {  // tensor-core instances
+    switch (cr) {
+      case 3: return launch_kernel<512, 3, 1>(num_sms, a, smem, st);
+      case 4: return launch_kernel<512, 4, 1>(num_sms, a, smem, st);
+      default: return launch_kernel<512, 5, 1>(num_sms, a, smem, st);
+    }
+  }
   if (threads == 512) {
     switch (cr) {
       case 2: return launch_kernel<512, 2>(num_sms, a, smem, st);

@@ -403,7 +403,8 @@ __device__ int block_purify(const double* F, int n, int nocc, double* X, double*
 }
 
 // ------------------------------------------------------------------------------------------
-// Mixed precision on the 5th-generation tensor cores (SOLVER_PURIFY_MIXED, 64 < n16 <= 128):
+// Mixed precision on the 5th-generation tensor cores (SOLVER_PURIFY_MIXED, 64 < n16 <= 128;
+// larger orders up to 160 go on to block_purify_mixed_wide below):
 // the products of the recursion run as tcgen05.mma kind::tf32 with the accumulator in tensor
 // memory, X split into two TF32 parts (hi = X with the low 13 mantissa bits cleared, lo = X - hi)
 // and X^2 ~ hi hi + hi lo + lo hi (FP32-level accuracy, "3xTF32").  hi and lo sit in shared
@@ -445,11 +446,29 @@ __device__ __forceinline__ void put_split(float* hi, float* lo, int idx, float v
   lo[idx] = v - h;
 }
 
+// Reads 16 consecutive accumulator columns of the warp's 32 tensor-memory lanes (one row per
+// thread); 16 at a time keeps the epilogue within the 128 registers a 512-thread CTA allows.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+        "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+        "=r"(v[14]), "=r"(v[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;");
+}
+
+template <int NT>
+__device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int nocc, double* X,
+                                                    double* lz, double* red);
+
 template <int NT>
 __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc, double* X,
                                                double* lz, double* red) {
   constexpr int NW = NT / 32;
   static_assert(NT == 512, "the tensor-memory epilogue maps 16 warps onto 4 x 4 tiles of 32");
+  if (purify_n16(n) > 128) return block_purify_mixed_wide<NT>(F, n, nocc, X, lz, red);
   const int ld = purify_ld(n), n16 = purify_n16(n);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double t1, t2;
@@ -540,28 +559,20 @@ __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc,
     }
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;");
-    uint32_t v[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
-        "%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
-          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
-          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;");
     double s1 = 0.0, s2 = 0.0;
-    if (row < n16) {
 #pragma unroll
-      for (int g = 0; g < 8; ++g) {  // four columns = 16 contiguous bytes of a core matrix row
-        const int c = c0 + 4 * g;
-        if (c < n16) {
+    for (int half = 0; half < 2; ++half) {
+      uint32_t v[16];
+      tmem_ld16(taddr + (uint32_t)(16 * half), v);
+#pragma unroll
+      for (int g = 0; g < 4; ++g) {  // four columns = 16 contiguous bytes of a core matrix row
+        const int c = c0 + 16 * half + 4 * g;
+        if (row < n16 && c < n16) {
           float h4[4], l4[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            const int j = 4 * g + q;
-            const float d = __uint_as_float(v[j]);
+            const int j = 16 * half + 4 * g + q;
+            const float d = __uint_as_float(v[4 * g + q]);
             const float nv = sq ? d : fmaf(2.0f, xr[j], -d);
             xr[j] = nv;
             h4[q] = __uint_as_float(__float_as_uint(nv) & 0xFFFFE000u);
@@ -632,6 +643,247 @@ __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc,
       X[r * ld + c] = back[e];
       if (r == c) s1 += back[e];
       s2 = fma(back[e], back[e], s2);
+    }
+  }
+  for (int t = threadIdx.x; t < n16 * 4; t += NT) X[(t >> 2) * ld + n16 + (t & 3)] = 0.0;  // pad
+  block_sum2<NT>(s1, s2, red);
+  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it);
+}
+
+// ------------------------------------------------------------------------------------------
+// The same mixed form for n16 = 144 and 160 (nao 129-160), where X is taller than one M = 128
+// tile.  hi / lo hold all n16 rows (2 x n16 x n16 floats inside X's region).  A product is two
+// accumulators: D1 = X[0:128, :] X (M = 128, N = n16, tensor-memory columns 0 .. n16-1) and
+// D2 = X[n16-128 : n16, :] X[:, 128 : n16] (M = 128, N = n16 - 128, columns kWideCorner ..),
+// whose last n16 - 128 rows are the corner X^2[128:n16, 128:n16].  The block
+// X^2[128:n16, 0:128] is the transpose of D1's columns 128 .. n16-1 (X^2 is symmetric), so the
+// warps that read those columns write each new element twice, at (r, c) and (c, r).  Tasks of
+// 32 rows x 32 columns: every warp one tile of D1[0:128, 0:128]; warps 0-3 also D1's fifth
+// column tile; warp 7 the corner from D2.  The old X of an element is read back from hi + lo.
+
+constexpr int kWideCorner = 192;  // tensor-memory column of D2 (256 columns allocated)
+
+// Row and column of the t-th element of a lower triangle stored row by row.
+__device__ __forceinline__ void tri_rc(int t, int& r, int& c) {
+  r = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+  while (r * (r + 1) / 2 > t) --r;
+  while ((r + 1) * (r + 2) / 2 <= t) ++r;
+  c = t - r * (r + 1) / 2;
+}
+
+// Half of a 32-column task of the wide epilogue: row `row` of X, columns cb .. cb + 15 (those
+// < n16), X^2 values in v.  Writes the new X into hi / lo at (row, c) and, with `mirror`, at (c, row);
+// adds to the trace and squared-norm sums (a mirrored element counts twice in the norm).
+__device__ __forceinline__ void wide_update(float* hi, float* lo, int n16, int row, int cb,
+                                            const uint32_t (&v)[16], bool sq, bool mirror,
+                                            double& s1, double& s2) {
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    const int c = cb + 4 * g;
+    if (c < n16) {
+      const int idx = kmajor_index(row, c, n16);
+      const float4 oh = *reinterpret_cast<const float4*>(hi + idx);
+      const float4 ol = *reinterpret_cast<const float4*>(lo + idx);
+      const float old[4] = {oh.x + ol.x, oh.y + ol.y, oh.z + ol.z, oh.w + ol.w};
+      float h4[4], l4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float d = __uint_as_float(v[4 * g + q]);
+        const float nv = sq ? d : fmaf(2.0f, old[q], -d);
+        h4[q] = __uint_as_float(__float_as_uint(nv) & 0xFFFFE000u);
+        l4[q] = nv - h4[q];
+        if (row == c + q) s1 += nv;
+        s2 = fma(mirror ? 2.0 * (double)nv : (double)nv, (double)nv, s2);
+        if (mirror) {
+          const int tdx = kmajor_index(c + q, row, n16);
+          hi[tdx] = h4[q];
+          lo[tdx] = l4[q];
+        }
+      }
+      *reinterpret_cast<float4*>(hi + idx) = make_float4(h4[0], h4[1], h4[2], h4[3]);
+      *reinterpret_cast<float4*>(lo + idx) = make_float4(l4[0], l4[1], l4[2], l4[3]);
+    }
+  }
+}
+
+template <int NT>
+__device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int nocc, double* X,
+                                                    double* lz, double* red) {
+  constexpr int NW = NT / 32;
+  static_assert(NT == 512, "the tensor-memory epilogue maps 16 warps onto 4 x 4 tiles of 32");
+  const int ld = purify_ld(n), n16 = purify_n16(n), R = n16 - 128;  // R = 16 or 32
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double t1, t2;
+  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+  // ---- X (FP64, lower triangle, row stride ld) -> hi / lo (both triangles) ----
+  float* hi = reinterpret_cast<float*>(X);
+  float* lo = hi + n16 * n16;
+  constexpr int kTri = (160 * 161 / 2 + NT - 1) / NT;
+  const int ntri = n16 * (n16 + 1) / 2;
+  float keep[kTri];
+#pragma unroll
+  for (int e = 0; e < kTri; ++e) {
+    const int t = threadIdx.x + e * NT;
+    keep[e] = 0.0f;
+    if (t < ntri) {
+      int r, c;
+      tri_rc(t, r, c);
+      keep[e] = (float)X[r * ld + c];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < kTri; ++e) {
+    const int t = threadIdx.x + e * NT;
+    if (t < ntri) {
+      int r, c;
+      tri_rc(t, r, c);
+      put_split(hi, lo, kmajor_index(r, c, n16), keep[e]);
+      if (r != c) put_split(hi, lo, kmajor_index(c, r, n16), keep[e]);
+    }
+  }
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(lz);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(lz + 1);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  if (warp == 0)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(256));
+  asm volatile("fence.proxy.async.shared::cta;");
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tslot;
+  const uint32_t id1 = umma_idesc_tf32(128, n16), id2 = umma_idesc_tf32(128, R);
+  const uint32_t lbo = 128, sbo = (uint32_t)(n16 / 4) * 128;
+  const uint32_t a2 = (uint32_t)(R / 8) * sbo, b2 = 16u * sbo;  // D2's first rows of A and B
+  const int quad = warp & 3, row = 32 * quad + lane, c0 = (warp >> 2) * 32;
+  const uint32_t tlane = (uint32_t)(32 * quad) << 16;
+  int it = 0, status = 0;
+  uint32_t phase = 0;
+  for (; it < kPurifyMaxIter; ++it) {
+    if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) { status = -1; break; }
+    if (fabs(t1 - t2) < kPurifyTensorSwitch) break;
+    const double n_o = (double)nocc;
+    const bool sq = fabs(t2 - n_o) < fabs(2.0 * t1 - t2 - n_o);
+    if (threadIdx.x == 0) {
+      const uint32_t h0 = smem_u32(hi), l0 = smem_u32(lo);
+      for (int acc = 0; acc < 2; ++acc) {
+        const uint32_t ao = acc ? a2 : 0u, bo = acc ? b2 : 0u, id = acc ? id2 : id1;
+        const uint32_t d = tmem + (acc ? (uint32_t)kWideCorner : 0u);
+        int first = 1;
+        for (int k0 = 0; k0 < n16; k0 += 8) {
+          const uint32_t off = (uint32_t)(k0 / 4) * 128;
+          const uint64_t ah = umma_smem_desc(h0 + ao + off, lbo, sbo);
+          const uint64_t al = umma_smem_desc(l0 + ao + off, lbo, sbo);
+          const uint64_t bh = umma_smem_desc(h0 + bo + off, lbo, sbo);
+          const uint64_t bl = umma_smem_desc(l0 + bo + off, lbo, sbo);
+          const uint64_t da[3] = {ah, ah, al}, db[3] = {bh, bl, bh};
+#pragma unroll
+          for (int q = 0; q < 3; ++q) {
+            asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
+                         "l"(da[q]), "l"(db[q]), "r"(id), "r"(first ? 0 : 1));
+            first = 0;
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(mbar)));
+    }
+    uint32_t done = 0;
+    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n\t}"
+                   : "=r"(done)
+                   : "r"(smem_u32(mbar)), "r"(phase));
+      if (!done) __nanosleep(64);
+    }
+    if (__syncthreads_or(!done)) {
+      status = -2;
+      break;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    double s1 = 0.0, s2 = 0.0;
+    const int xr = n16 - 32 + lane;  // warp 7 (quadrant 3 of D2): lane l is row n16 - 32 + l
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const uint32_t h16 = (uint32_t)(16 * half);
+      uint32_t v[16];
+      tmem_ld16(tmem + tlane + (uint32_t)c0 + h16, v);
+      wide_update(hi, lo, n16, row, c0 + 16 * half, v, sq, false, s1, s2);
+      if (warp < 4) {  // D1's columns 128 .. n16-1: rows < 128 here, rows >= 128 by symmetry
+        tmem_ld16(tmem + tlane + 128u + h16, v);
+        wide_update(hi, lo, n16, row, 128 + 16 * half, v, sq, true, s1, s2);
+      }
+      if (warp == 7) {
+        tmem_ld16(tmem + tlane + (uint32_t)kWideCorner + h16, v);
+        if (xr >= 128) wide_update(hi, lo, n16, xr, 128 + 16 * half, v, sq, false, s1, s2);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    double* part = red + 32 * (it & 1);
+    if (lane == 0) { part[warp] = s1; part[16 + warp] = s2; }
+    asm volatile("fence.proxy.async.shared::cta;");
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();  // X rewritten, tensor memory read: the next product may start
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    s1 = 0.0;
+    s2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) { s1 += part[k]; s2 += part[16 + k]; }
+    t1 = s1;
+    t2 = s2;
+  }
+  if (status == -2) {
+    uint32_t done = 0;
+    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+      asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                   "selp.u32 %0, 1, 0, p;\n\t}"
+                   : "=r"(done)
+                   : "r"(smem_u32(mbar)), "r"(phase));
+      if (!done) __nanosleep(64);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(mbar)));
+  if (status < 0) return -1;
+  if (it == kPurifyMaxIter) return -1;
+  // ---- back to FP64 (lower triangle averaged with the upper, written to both) ----
+  double back[kTri];
+#pragma unroll
+  for (int e = 0; e < kTri; ++e) {
+    const int t = threadIdx.x + e * NT;
+    back[e] = 0.0;
+    if (t < ntri) {
+      int r, c;
+      tri_rc(t, r, c);
+      const int a = kmajor_index(r, c, n16), b = kmajor_index(c, r, n16);
+      back[e] = 0.5 * (((double)hi[a] + (double)lo[a]) + ((double)hi[b] + (double)lo[b]));
+    }
+  }
+  __syncthreads();
+  double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+  for (int e = 0; e < kTri; ++e) {
+    const int t = threadIdx.x + e * NT;
+    if (t < ntri) {
+      int r, c;
+      tri_rc(t, r, c);
+      X[r * ld + c] = back[e];
+      X[c * ld + r] = back[e];
+      if (r == c) s1 += back[e];
+      s2 = fma(r == c ? back[e] : 2.0 * back[e], back[e], s2);
     }
   }
   for (int t = threadIdx.x; t < n16 * 4; t += NT) X[(t >> 2) * ld + n16 + (t & 3)] = 0.0;  // pad

@@ -135,7 +135,7 @@ def test_diis_converges_to_the_same_energy_in_no_more_steps():
 
 
 def test_mixed_tensor_core_products_in_batch(gpu_ctx):
-    """Mixed form in the batch: nao 65-128 purify with TF32 tcgen05 products (3xTF32) and an FP64
+    """Mixed form in the batch: nao 65-128 (one 128-row tile) purify with TF32 tcgen05 products (3xTF32) and an FP64
     finish; every molecule converges within 1e-4 eV of the FP64 form, without a fallback."""
     rng = np.random.default_rng(17)
     mols = [geo.alkane(k, rng) for k in (11, 13, 15, 17, 19, 21)]  # nao 68 .. 128
@@ -156,3 +156,28 @@ def test_mixed_tensor_core_products_in_batch(gpu_ctx):
     assert np.all(r["status"] == 0) and np.all(r["converged"])
     assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
     np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
+
+
+def test_mixed_tensor_core_products_two_accumulators(gpu_ctx):
+    """nao 129-160 (n16 144 and 160): X taller than one 128-row tile, products from two
+    tensor-memory accumulators plus symmetry; same bar as the single-tile form."""
+    rng = np.random.default_rng(23)
+    mols = [geo.alkane(k, rng) for k in (22, 23, 24, 25, 26)]  # nao 134 .. 158
+    mols += [geo.polyene(k, rng) for k in (26, 28, 30)]         # nao 132 .. 152
+    assert {(m.nao + 15) // 16 * 16 for m in mols} == {144, 160}
+    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ctx = sg.Context(0)
+    try:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        b = sg.Batch(ctx, mols)
+        b.set_profiling(True)
+        b.run(1e-6)
+        r = b.results()
+        sc = b.stage_cycles()
+        b.close()
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
+    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
+    assert np.all(np.abs(r["n_iter"] - ref["n_iter"]) <= 1)
