@@ -405,6 +405,18 @@ def run_ours(args):
         served = serving.stats(srv_done)
         served.update({"rate_per_s": srate, "duration_s": sdur, "slots": 3,
                        "composition": "as the batch (seeded), open-loop Poisson arrivals"})
+        # the same stream served in mixed precision, each result against its FP64 one
+        srv = serving.Server(device=local, slots=3, hbm_budget=12 << 30, tol=TOL,
+                             solver=sg.SOLVER_PURIFY_MIXED)
+        try:
+            srv.replay([(0.001 * i, m) for i, m in enumerate(smols[-64:])])  # warm-up
+            mix_done = srv.replay(arrivals)
+        finally:
+            srv.close()
+        served_mixed = serving.stats(mix_done)
+        served_mixed["max_abs_dE_total_eV"] = float(max(
+            abs(a.result["E_tot"] - b.result["E_tot"]) for a, b in zip(mix_done, srv_done)))
+        served_mixed["precision"] = "TF32 tcgen05 products for nao 65-160, FP64 finish"
         # CPU baseline: the reference build on the host cores, bounded sample
         cpu = None
         if reference_kind():
@@ -432,6 +444,7 @@ def run_ours(args):
                            "definition": "per-molecule time from launch start to its converged "
                                          "energy, device clock"},
             "mixed_precision": mixed,
+            "serving_mixed": served_mixed,
             "plain_fp64_gpu": {"value": plain, "unit": UNIT,
                                "p50_ms": 1e3 * statistics.median(plain_lat),
                                "p99_ms": 1e3 * float(np.percentile(plain_lat, 99)),

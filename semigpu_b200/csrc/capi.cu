@@ -105,6 +105,11 @@ struct sgb_ctx {
   std::vector<std::pair<char*, size_t>> spare;
   size_t spare_bytes = 0;
   std::mutex spare_mutex;
+  // pinned host buffer for copies between caller memory and the device (upload / download)
+  char* staging = nullptr;
+  size_t staging_bytes = 0;
+  cudaEvent_t staging_ev = nullptr;  // recorded after the last uploads read from it
+  bool staging_busy = false;
 };
 
 struct sgb_batch {
@@ -303,6 +308,87 @@ void arena_put(sgb_ctx* ctx, char* p, size_t bytes) {
   release_spares(ctx, kSpareMaxBlocks, kSpareMaxBytes);
 }
 
+// ---- host staging ----
+// A cudaMemcpyAsync to or from pageable memory is staged by the driver, and such a copy was seen
+// to wait behind another host thread's pending pageable copy: a 1 KB read-back held up for the
+// 2 s of another context's launch.  The copies between caller memory and the device therefore go
+// through the context's own pinned buffer (plain DMA on its stream); memory the caller pinned
+// is copied directly.
+constexpr size_t kStagingBytes = size_t(8) << 20;
+
+struct HostCopy {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+
+bool host_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
+size_t staged_bytes(const HostCopy* c, int n) {
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) total += (c[i].bytes + 15) & ~size_t(15);
+  return total;
+}
+
+// Host -> device copies on st.  Staged sources are copied into the buffer at once, so the
+// caller's memory may be reused on return; the buffer is reused only after these copies ran.
+cudaError_t upload(sgb_ctx* ctx, const HostCopy* c, int n, cudaStream_t st) {
+  const bool stage = ctx->staging && staged_bytes(c, n) <= ctx->staging_bytes;
+  cudaError_t e;
+  if (stage && ctx->staging_busy && (e = cudaEventSynchronize(ctx->staging_ev)) != cudaSuccess)
+    return e;
+  size_t off = 0;
+  for (int i = 0; i < n; ++i) {
+    if (!c[i].bytes) continue;
+    if (stage && !host_pinned(c[i].src)) {
+      memcpy(ctx->staging + off, c[i].src, c[i].bytes);
+      e = cudaMemcpyAsync(c[i].dst, ctx->staging + off, c[i].bytes, cudaMemcpyHostToDevice, st);
+      off += (c[i].bytes + 15) & ~size_t(15);
+    } else {
+      e = cudaMemcpyAsync(c[i].dst, c[i].src, c[i].bytes, cudaMemcpyHostToDevice, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  if (off) {
+    if ((e = cudaEventRecord(ctx->staging_ev, st)) != cudaSuccess) return e;
+    ctx->staging_busy = true;
+  }
+  return cudaSuccess;
+}
+
+// Device -> host copies on st; returns when they have landed in the caller's memory.
+cudaError_t download(sgb_ctx* ctx, const HostCopy* c, int n, cudaStream_t st) {
+  const bool stage = ctx->staging && staged_bytes(c, n) <= ctx->staging_bytes;
+  cudaError_t e;
+  if (stage && ctx->staging_busy && (e = cudaEventSynchronize(ctx->staging_ev)) != cudaSuccess)
+    return e;
+  size_t off = 0;
+  std::vector<size_t> at(n, ~size_t(0));
+  for (int i = 0; i < n; ++i) {
+    if (!c[i].bytes || !c[i].dst) continue;
+    if (stage && !host_pinned(c[i].dst)) {
+      at[i] = off;
+      e = cudaMemcpyAsync(ctx->staging + off, c[i].src, c[i].bytes, cudaMemcpyDeviceToHost, st);
+      off += (c[i].bytes + 15) & ~size_t(15);
+    } else {
+      e = cudaMemcpyAsync(c[i].dst, c[i].src, c[i].bytes, cudaMemcpyDeviceToHost, st);
+    }
+    if (e != cudaSuccess) return e;
+  }
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  ctx->staging_busy = false;
+  for (int i = 0; i < n; ++i)
+    if (at[i] != ~size_t(0)) memcpy(c[i].dst, ctx->staging + at[i], c[i].bytes);
+  return cudaSuccess;
+}
+
 void free_batch(sgb_batch* b) {
   if (!b) return;
   if (b->arena && b->from_pool) {
@@ -451,16 +537,14 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->d_stage = (unsigned long long*)(base + o_stage);
   b->d_hist = hist_stride > 0 ? (double*)(base + o_hist) : nullptr;
   cudaStream_t st = ctx->stream;
-  auto up = [&](void* dst, const void* src, size_t bytes) {
-    return bytes ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
-  };
-  if ((e = up(b->d_desc, b->desc.data(), sizeof(MolDesc) * nmol)) != cudaSuccess ||
-      (e = up(b->d_order, b->order.data(), sizeof(int) * nmol)) != cudaSuccess ||
-      (e = up(b->d_slot, slot.data(), NA)) != cudaSuccess ||
-      (e = up(b->d_xyz, xyz, 24 * NA)) != cudaSuccess ||
-      (e = up(b->d_first, first.data(), 4 * NA)) != cudaSuccess ||
-      (e = up(b->d_row_off, row_off.data(), 8 * NA)) != cudaSuccess ||
-      (e = up(b->d_hb, hb.data(), 4 * NA)) != cudaSuccess ||
+  const HostCopy ups[] = {{b->d_desc, b->desc.data(), sizeof(MolDesc) * nmol},
+                          {b->d_order, b->order.data(), sizeof(int) * (size_t)nmol},
+                          {b->d_slot, slot.data(), (size_t)NA},
+                          {b->d_xyz, xyz, 24 * (size_t)NA},
+                          {b->d_first, first.data(), 4 * (size_t)NA},
+                          {b->d_row_off, row_off.data(), 8 * (size_t)NA},
+                          {b->d_hb, hb.data(), 4 * (size_t)NA}};
+  if ((e = upload(ctx, ups, 7, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->d_status, 0, 4 * nmol, st)) != cudaSuccess ||
       (e = take_event(ctx, &b->ev0)) != cudaSuccess || (e = take_event(ctx, &b->ev1)) != cudaSuccess) {
     free_batch(b);
@@ -1198,6 +1282,13 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   int optin = 0;
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
   c->smem_optin = optin;
+  if (cudaHostAlloc(&c->staging, kStagingBytes, cudaHostAllocDefault) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->staging_ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    sgb_ctx_destroy(c);
+    return SGB_E_CUDA;
+  }
+  c->staging_bytes = kStagingBytes;
   for (int k = 0; k < 8; ++k) {
     cudaEvent_t ev;
     if (cudaEventCreate(&ev) != cudaSuccess) {
@@ -1308,6 +1399,9 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
     if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);
   }
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // staged copies may still be running
+  if (ctx->staging) cudaFreeHost(ctx->staging);
+  if (ctx->staging_ev) cudaEventDestroy(ctx->staging_ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   for (cudaEvent_t ev : ctx->events) cudaEventDestroy(ev);
   delete ctx;
@@ -1506,7 +1600,8 @@ int sgb_batch_destroy(sgb_batch* b) {
 int sgb_batch_set_coordinates(sgb_ctx* ctx, sgb_batch* b, const double* xyz) {
   if (!ctx || !b || !xyz) return SGB_E_ARG;
   const int64_t NA = b->natoms_total;
-  CUDA_TRY(ctx, cudaMemcpyAsync(b->d_xyz, xyz, 24 * NA, cudaMemcpyHostToDevice, ctx->stream));
+  const HostCopy up = {b->d_xyz, xyz, 24 * (size_t)NA};
+  CUDA_TRY(ctx, upload(ctx, &up, 1, ctx->stream));
   k_ang_to_bohr<<<std::max<int64_t>(1, std::min<int64_t>((3 * NA + 255) / 256, 1024)), 256, 0,
                   ctx->stream>>>(b->d_xyz, b->d_pos, 3 * NA);
   CUDA_TRY(ctx, cudaGetLastError());
@@ -1521,14 +1616,13 @@ int sgb_batch_run(sgb_ctx* ctx, sgb_batch* b, double tol, int max_iter) {
 int sgb_batch_results(sgb_ctx* ctx, sgb_batch* b, double* e_el, double* e_cc, int* n_iter,
                       int* converged, int* status) {
   if (!ctx || !b) return SGB_E_ARG;
-  cudaStream_t st = ctx->stream;
-  const int n = b->nmol;
-  if (e_el) CUDA_TRY(ctx, cudaMemcpyAsync(e_el, b->d_eel, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
-  if (e_cc) CUDA_TRY(ctx, cudaMemcpyAsync(e_cc, b->d_ecc, 8 * (size_t)n, cudaMemcpyDeviceToHost, st));
-  if (n_iter) CUDA_TRY(ctx, cudaMemcpyAsync(n_iter, b->d_niter, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
-  if (converged) CUDA_TRY(ctx, cudaMemcpyAsync(converged, b->d_conv, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
-  if (status) CUDA_TRY(ctx, cudaMemcpyAsync(status, b->d_status, 4 * (size_t)n, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  const size_t n = (size_t)b->nmol;
+  const HostCopy downs[] = {{e_el, b->d_eel, e_el ? 8 * n : 0},
+                            {e_cc, b->d_ecc, e_cc ? 8 * n : 0},
+                            {n_iter, b->d_niter, n_iter ? 4 * n : 0},
+                            {converged, b->d_conv, converged ? 4 * n : 0},
+                            {status, b->d_status, status ? 4 * n : 0}};
+  CUDA_TRY(ctx, download(ctx, downs, 5, ctx->stream));
   CUDA_TRY(ctx, cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1));
   return SGB_OK;
 }
@@ -1543,9 +1637,10 @@ int sgb_batch_timestamps(sgb_ctx* ctx, sgb_batch* b, unsigned long long* t_begin
                          unsigned long long* t_end) {
   if (!ctx || !b) return SGB_E_ARG;
   const size_t n = (size_t)b->nmol;
-  if (t_begin) CUDA_TRY(ctx, cudaMemcpyAsync(t_begin, b->d_tb, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
-  if (t_end) CUDA_TRY(ctx, cudaMemcpyAsync(t_end, b->d_te, 8 * n, cudaMemcpyDeviceToHost, ctx->stream));
-  return sgb_ctx_synchronize(ctx);
+  const HostCopy downs[] = {{t_begin, b->d_tb, t_begin ? 8 * n : 0},
+                            {t_end, b->d_te, t_end ? 8 * n : 0}};
+  CUDA_TRY(ctx, download(ctx, downs, 2, ctx->stream));
+  return SGB_OK;
 }
 
 int sgb_batch_launches(const sgb_batch* b, int* launches) {
@@ -1565,9 +1660,9 @@ int sgb_batch_set_profiling(sgb_batch* b, int on) {
 int sgb_batch_stage_cycles(sgb_ctx* ctx, sgb_batch* b, unsigned long long* cycles) {
   if (!ctx || !b || !cycles) return SGB_E_ARG;
   if (!b->profiling) return fail(ctx, SGB_E_STATE, "stage timers are off (sgb_batch_set_profiling)");
-  CUDA_TRY(ctx, cudaMemcpyAsync(cycles, b->d_stage, 8 * (size_t)kStageSlots * b->nmol,
-                                cudaMemcpyDeviceToHost, ctx->stream));
-  return sgb_ctx_synchronize(ctx);
+  const HostCopy down = {cycles, b->d_stage, 8 * (size_t)kStageSlots * b->nmol};
+  CUDA_TRY(ctx, download(ctx, &down, 1, ctx->stream));
+  return SGB_OK;
 }
 
 int sgb_batch_device_coordinates(sgb_batch* b, void** dptr) {

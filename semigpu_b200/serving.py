@@ -14,6 +14,9 @@ queues, and `big_slots` of the workers serve only the large queue, so a small re
 waits for a batch that holds a large molecule.  Molecules above nao 1024 run through the
 single-molecule grid path in the large-queue worker that picked them.
 
+`solver` picks how each SCF step gets the density (SOLVER_PURIFY, the FP64 default, or
+SOLVER_PURIFY_MIXED: TF32 tensor-core products with an FP64 finish, within 1e-4 eV of FP64).
+
 Latency of a request = completion time - arrival time (host clock); `stats()` reports p50/p99
 and throughput.  `replay()` drives an open-loop arrival schedule (e.g. Poisson) in real time.
 """
@@ -26,7 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import Context, Molecule, run_molecules
+from . import SOLVER_PURIFY, SOLVER_PURIFY_MIXED, Context, Molecule, run_molecules
 from .geometry import Molecule as Geometry
 
 CTA_MAX_NAO = 1024  # larger molecules take the grid path
@@ -62,12 +65,14 @@ class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
                  batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
-                 big_sm_share: float = 0.6):
+                 big_sm_share: float = 0.6, solver: int | None = None):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
         queue of molecules above nao 160 (at least one slot stays with the small queue); their
         launches together use at most big_sm_share of the SMs, so the persistent large-molecule
-        launches (seconds) always leave SMs to the small ones."""
+        launches (seconds) always leave SMs to the small ones.  solver: the density solver of
+        every worker context (None: the library default)."""
+        self.solver = solver
         self.big_sm_share = big_sm_share
         self.tol, self.max_iter = tol, max_iter
         self.max_batch = max_batch
@@ -120,14 +125,17 @@ class Server:
             w.join(timeout=60)
 
     def replay(self, arrivals, time_scale: float = 1.0) -> list[Request]:
-        """Submits (t, molecule) pairs at their arrival times (open loop) and waits for all."""
+        """Submits (t, molecule) pairs at their arrival times (open loop), waits for all and
+        returns this replay's requests (earlier ones, e.g. a warm-up, are left out)."""
+        with self._cv:
+            first = self._next
         t0 = time.perf_counter()
         for t, mol in arrivals:
             delay = t0 + t * time_scale - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
             self.submit(mol, t_arrival=t0 + t * time_scale)
-        return self.drain()
+        return [r for r in self.drain() if r.rid >= first]
 
     # -- worker side ------------------------------------------------------------------------
     def _take(self, queue) -> list[Request]:
@@ -148,6 +156,8 @@ class Server:
         try:
             if self.engine is run_molecules:
                 ctx = Context(self._device)
+                if self.solver is not None:
+                    ctx.set_density_solver(self.solver)
                 if big and self.big_slots:
                     ctx.set_sm_share(max(0.05, self.big_sm_share / self.big_slots))
                 # batches are built in a per-worker arena: no cudaMalloc/cudaFree per batch
@@ -235,6 +245,8 @@ def main(argv=None):
     ap.add_argument("--big-slots", type=int, default=2)
     ap.add_argument("--hbm-gb", type=float, default=40.0)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--mixed", action="store_true",
+                    help="mixed precision (TF32 tensor-core products, FP64 finish)")
     args = ap.parse_args(argv)
     if args.workload == "c5":
         arrivals = geo.serving_c5(rate=args.rate, duration_s=args.duration, seed=args.seed)
@@ -247,13 +259,15 @@ def main(argv=None):
                 break
             times.append(t)
         arrivals = list(zip(times, geo.batch_c3(len(times), seed=args.seed)))
-    srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)))
+    srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)),
+                 solver=SOLVER_PURIFY_MIXED if args.mixed else SOLVER_PURIFY)
     try:
         srv.replay([(0.001 * i, m) for i, (_, m) in enumerate(arrivals[:40])])  # warm-up
         done = srv.replay(arrivals)
     finally:
         srv.close()
     out = {"workload": args.workload, "rate_per_s": args.rate, "duration_s": args.duration,
+           "precision": "mixed" if args.mixed else "fp64",
            "all": stats(done),
            "small": stats([r for r in done if r.mol.nao <= SMEM_MAX_NAO]),
            "large": stats([r for r in done if r.mol.nao > SMEM_MAX_NAO]),

@@ -116,3 +116,31 @@ def test_served_results_equal_alone():
             assert abs(done[i].result["E_tot"] - alone["E_tot"]) < 1e-9
     s = serving.stats(done)
     assert s["all_converged"] and s["p99_ms"] > 0
+
+
+@pytest.mark.gpu
+def test_served_mixed_precision_within_tolerance_of_fp64():
+    """Serving in mixed precision (TF32 tensor-core products, FP64 finish): each result equals
+    the same molecule run alone in mixed precision, and is within 1e-4 eV of FP64."""
+    import semigpu_b200 as sg
+
+    mols = geo.batch_c3(96, seed=22)
+    srv = serving.Server(slots=3, hbm_budget=2 << 30, solver=sg.SOLVER_PURIFY_MIXED)
+    try:
+        done = srv.replay([(0.0005 * i, m) for i, m in enumerate(mols)])
+    finally:
+        srv.close()
+    assert len(done) == 96 and all(r.result["status"] == 0 for r in done)
+    assert serving.stats(done)["all_converged"]
+    with sg.Context(0) as c64:
+        fp64 = sg.run_molecules(c64, mols, tol=1e-6)
+    e = np.array([r.result["E_tot"] for r in done])
+    np.testing.assert_allclose(e, fp64["E_tot"], rtol=0, atol=1e-4)
+    big = [i for i, m in enumerate(mols) if 64 < m.nao <= 160][:4]
+    assert big  # the tensor-core form is exercised
+    with sg.Context(0) as ctx:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        for i in big:
+            alone = sg.Molecule.from_geometry(ctx, mols[i]).run(tol=1e-6)
+            assert done[i].result["n_iter"] == alone["n_iter"]
+            assert abs(done[i].result["E_tot"] - alone["E_tot"]) < 1e-9
