@@ -13,8 +13,8 @@
 // element sums of the current one, before its product starts.
 //
 // X lives in shared memory: n16 x n16 (nao rounded up to 16, zero padding, which stays zero),
-// row stride n16 + 4 doubles (8 rows x 4 columns of a fragment load then fall in distinct banks
-// within each half-warp phase).  The product's lower triangle is tiled in 16 x 16 super-tiles,
+// row stride n16 + 8 doubles (the two rows of a quarter-warp's 16-byte fragment loads fall in
+// opposite halves of the banks).  The product's lower triangle is tiled in 16 x 16 super-tiles,
 // dealt round-robin to the warps; each warp keeps its accumulators in registers until every
 // warp has finished reading X, then writes the new X (lower triangle and its mirror) in place.
 //
@@ -134,7 +134,7 @@ __host__ __device__ inline void lanczos_bounds(const double* a, const double* b,
 }
 
 __host__ __device__ inline int purify_n16(int n) { return (n + 15) & ~15; }
-__host__ __device__ inline int purify_ld(int n) { return purify_n16(n) + 4; }
+__host__ __device__ inline int purify_ld(int n) { return purify_n16(n) + 8; }
 __host__ __device__ inline size_t purify_doubles(int n) {
   return (size_t)purify_n16(n) * (size_t)purify_ld(n);
 }
@@ -300,21 +300,32 @@ __device__ __noinline__ void purify_step(double* X, int n16, int ld, bool sq, do
   for (int u = 0; u < MAXST; ++u) {
     int I = 0, J = 0;
     if (warp + u * NW < cnt) tri_inverse(warp + u * NW, I, J);
-    rowI[u] = (I * 16 + g) * ld + q;
-    rowJ[u] = (J * 16 + g) * ld + q;
+    rowI[u] = (I * 16 + g) * ld + 2 * q;
+    rowJ[u] = (J * 16 + g) * ld + 2 * q;
 #pragma unroll
     for (int k = 0; k < 4; ++k) acc[u][k][0] = acc[u][k][1] = 0.0;
   }
-  for (int k0 = 0; k0 < n16; k0 += 4) {
+  // Lane (g, q) loads columns k0 + 2q, k0 + 2q + 1 of its rows as one 16-byte load; the first
+  // DMMA takes the even columns, the second the odd ones (the same permutation of k for A and
+  // B, so the sum is unchanged).  Row stride ld = n16 + 8 keeps a quarter-warp's two rows in
+  // opposite halves of the banks.
+  for (int k0 = 0; k0 < n16; k0 += 8) {
 #pragma unroll
     for (int u = 0; u < MAXST; ++u) {
       if (warp + u * NW < cnt) {
-        const double a0 = X[rowI[u] + k0], a1 = X[rowI[u] + 8 * ld + k0];
-        const double b0 = X[rowJ[u] + k0], b1 = X[rowJ[u] + 8 * ld + k0];
-        dmma884(acc[u][0][0], acc[u][0][1], a0, b0);
-        if (rowI[u] != rowJ[u]) dmma884(acc[u][1][0], acc[u][1][1], a0, b1);
-        dmma884(acc[u][2][0], acc[u][2][1], a1, b0);
-        dmma884(acc[u][3][0], acc[u][3][1], a1, b1);
+        const double2 a0 = *reinterpret_cast<const double2*>(X + rowI[u] + k0);
+        const double2 a1 = *reinterpret_cast<const double2*>(X + rowI[u] + 8 * ld + k0);
+        const double2 b0 = *reinterpret_cast<const double2*>(X + rowJ[u] + k0);
+        const double2 b1 = *reinterpret_cast<const double2*>(X + rowJ[u] + 8 * ld + k0);
+        const bool off = rowI[u] != rowJ[u];
+        dmma884(acc[u][0][0], acc[u][0][1], a0.x, b0.x);
+        if (off) dmma884(acc[u][1][0], acc[u][1][1], a0.x, b1.x);
+        dmma884(acc[u][2][0], acc[u][2][1], a1.x, b0.x);
+        dmma884(acc[u][3][0], acc[u][3][1], a1.x, b1.x);
+        dmma884(acc[u][0][0], acc[u][0][1], a0.y, b0.y);
+        if (off) dmma884(acc[u][1][0], acc[u][1][1], a0.y, b1.y);
+        dmma884(acc[u][2][0], acc[u][2][1], a1.y, b0.y);
+        dmma884(acc[u][3][0], acc[u][3][1], a1.y, b1.y);
       }
     }
   }
@@ -891,7 +902,7 @@ __device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int 
   return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it);
 }
 
-// Above nao 160 X does not fit in shared memory: X and Y (n16 x n16, row stride n16 + 4) live
+// Above nao 160 X does not fit in shared memory: X and Y (n16 x n16, row stride n16 + 8) live
 // in global memory (L1/L2-resident panels).  A warp takes one super-tile at a time, keeps its
 // four 8 x 8 accumulators in registers and writes the new values straight into Y, reading the
 // old X for the 2X - X^2 branch; the caller swaps X and Y after each step.
