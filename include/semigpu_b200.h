@@ -90,12 +90,13 @@ int sgb_ctx_set_class_threads(sgb_ctx *ctx, int count, const int *threads);
  * server running several contexts side by side uses it so that one context's persistent
  * launch of long (large-molecule) work leaves SMs to the others. */
 int sgb_ctx_set_sm_share(sgb_ctx *ctx, double share);
-/* Pulay DIIS of depth 2..8 (0 = off, the default) for the single-molecule SCF on the whole GPU
- * (the grid path, nao > 160 by default): F is extrapolated from the last `depth` Fock matrices
- * with the commutator FP - PF as error.  It changes the SCF trajectory, so step counts no
- * longer follow the reference's; the converged energy is the same.  Next step after the
- * reference's SCF loop (scfcalculation.cpp:82-141), which has no convergence acceleration;
- * the batched path does not use it. */
+/* Pulay DIIS of depth 2..8 (0 = off, the default) for every SCF of this context: F is
+ * extrapolated from the last `depth` Fock matrices: on the grid path by the host, with the
+ * commutator FP - PF as error; in the batched launches, and single molecules on one CTA, by
+ * each molecule's CTA, with the Fock residual F(P_k) - F_k as error (no dense product per step)
+ * and (2 depth + 1) nao^2 doubles of history per molecule allocated on the first such launch.  It changes the SCF trajectory, so step counts no longer follow the
+ * reference's; the converged energy is the same.  Next step after the reference's SCF loop
+ * (scfcalculation.cpp:82-141), which has no convergence acceleration. */
 int sgb_ctx_set_diis(sgb_ctx *ctx, int depth);
 /* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
  * it instead of allocating, and releasing the batch does not free device memory (cudaFree

@@ -170,7 +170,8 @@ class Context:
         self.check(lib().sgb_ctx_set_class_threads(self.h, len(t), _i(t)), "set_class_threads")
 
     def set_diis(self, depth: int):
-        """Pulay DIIS of this depth (0 = off) for single-molecule runs on the grid path."""
+        """Pulay DIIS of this depth (2..8; 0 = off) for this context's SCF runs (batched
+        launches and single molecules alike); step counts then differ from the reference's."""
         self.check(lib().sgb_ctx_set_diis(self.h, int(depth)), "set_diis")
 
     def set_sm_share(self, share: float):

@@ -62,6 +62,11 @@ struct BatchArgs {
   unsigned long long* t_begin;  // optional per-molecule %globaltimer (ns) at start / end
   unsigned long long* t_end;
   unsigned long long* stage_cycles;  // optional, kStageSlots SM cycles per molecule
+  // Pulay DIIS (launched only with it on): (2 depth + 1) n^2 doubles of history per molecule
+  // at (2 depth + 1) sq0, and kDiisB doubles of B matrix per molecule
+  double* diis = nullptr;
+  double* diis_B = nullptr;
+  int diis_depth = 0;
 };
 
 // Stage timers (SM clock cycles of the CTA, thread 0, between block-wide barriers), the
@@ -243,6 +248,116 @@ __device__ inline void split_by_rank(const double* dval, int n, int nocc, int* o
 // PLACE: 0 = G and V in shared memory (nao <= kVsmemMax), 1 = G in shared memory and V in
 // global memory (nao <= kGsmemMax), 2 = both in global memory (larger; CR must be 0).  A
 // template parameter so every access in the eigensolver has a known address space.
+// ---- Pulay DIIS on the batched path (kernel instances with FEAT_DIIS; off by default) ----
+// The last diis_depth Fock matrices F_out(P_k) and their residuals e_k = F_out(P_k) - F_in,k
+// (F_in,k the matrix P_k was purified from) are kept in global memory; B_ij = <e_i, e_j>.  After
+// each Fock build the next density is purified from F = sum c_i F_out,i with
+// [B 1; 1 0] (c, -lambda) = (0, 1), solved by one thread (Gaussian elimination with partial
+// pivoting, B scaled by its largest diagonal); a singular system or a coefficient beyond 1e6
+// keeps the plain F.  The solve is the grid path's (capi.cu diis_step); the error vector is the
+// Fock residual (Pulay mixing of Fock matrices) instead of the commutator F P - P F, which
+// would need a dense product per step: with it each step cost 1.7x, more than the 38 % fewer
+// steps saved.  Both vanish at self-consistency.
+constexpr int kDiisMaxDepth = 8;
+constexpr int kDiisB = kDiisMaxDepth * kDiisMaxDepth;
+
+// Where a molecule's DIIS history starts: depth F_out, depth residuals, then F_in.
+__device__ __forceinline__ double* diis_history(const BatchArgs& a, int64_t sq0) {
+  return a.diis + (2 * (int64_t)a.diis_depth + 1) * sq0;
+}
+
+template <int NT>
+__device__ __noinline__ void block_diis(const BatchArgs& a, int64_t sq0, const MolView& m,
+                                        int mi, double* Ffull, int& count, int& next,
+                                        double* red) {
+  const int n = m.nao, depth = a.diis_depth;
+  const int64_t nn = (int64_t)n * n;
+  double* Fh = diis_history(a, sq0);
+  double* Eh = Fh + (int64_t)depth * nn;
+  double* Fin = Eh + (int64_t)depth * nn;
+  double* B = a.diis_B + (int64_t)mi * kDiisB;
+  const int slot = next;
+  double* Fs = Fh + slot * nn;
+  double* Es = Eh + slot * nn;
+  for (int64_t t = threadIdx.x; t < nn; t += NT) {
+    const double f = Ffull[t];
+    Fs[t] = f;
+    Es[t] = f - Fin[t];
+  }
+  __syncthreads();
+  count = count + 1 < depth ? count + 1 : depth;
+  next = (slot + 1) % depth;
+  for (int jj = 0; jj < count; ++jj) {
+    const double* Ej = Eh + jj * nn;
+    double s = 0.0, unused = 0.0;
+    for (int64_t t = threadIdx.x; t < nn; t += NT) s = fma(Es[t], Ej[t], s);
+    block_sum2<NT>(s, unused, red);
+    if (threadIdx.x == 0) B[slot * kDiisMaxDepth + jj] = B[jj * kDiisMaxDepth + slot] = s;
+  }
+  __syncthreads();
+  const int mm = count;
+  if (mm < 2) {
+    for (int64_t t = threadIdx.x; t < nn; t += NT) Fin[t] = Ffull[t];
+    __syncthreads();
+    return;
+  }
+  if (threadIdx.x == 0) {
+    double A[kDiisMaxDepth + 1][kDiisMaxDepth + 2];
+    double scale = 0.0;
+    for (int i = 0; i < mm; ++i) scale = fmax(scale, B[i * kDiisMaxDepth + i]);
+    bool ok = scale > 0.0;
+    for (int i = 0; i <= mm; ++i)
+      for (int k = 0; k <= mm + 1; ++k) A[i][k] = 0.0;
+    for (int i = 0; i < mm && ok; ++i) {
+      for (int j = 0; j < mm; ++j) A[i][j] = B[i * kDiisMaxDepth + j] / scale;
+      A[i][mm] = A[mm][i] = 1.0;
+    }
+    A[mm][mm + 1] = 1.0;
+    for (int c = 0; c <= mm && ok; ++c) {
+      int piv = c;
+      for (int r = c + 1; r <= mm; ++r)
+        if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+      if (!(fabs(A[piv][c]) > 1e-14)) { ok = false; break; }
+      for (int k = 0; k <= mm + 1; ++k) {
+        const double t = A[c][k];
+        A[c][k] = A[piv][k];
+        A[piv][k] = t;
+      }
+      for (int r = 0; r <= mm; ++r) {
+        if (r == c) continue;
+        const double f = A[r][c] / A[c][c];
+        for (int k = c; k <= mm + 1; ++k) A[r][k] -= f * A[c][k];
+      }
+    }
+    for (int i = 0; i < mm && ok; ++i) {
+      red[i] = A[i][mm + 1] / A[i][i];
+      if (!(fabs(red[i]) < 1e6)) ok = false;
+    }
+    red[kDiisMaxDepth] = ok ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const bool ok = red[kDiisMaxDepth] != 0.0;
+  double c[kDiisMaxDepth];
+#pragma unroll
+  for (int i = 0; i < kDiisMaxDepth; ++i) c[i] = i < mm ? red[i] : 0.0;
+  __syncthreads();  // red is reused by the next reduction
+  for (int64_t t = threadIdx.x; t < nn; t += NT) {
+    double f = Ffull[t];
+    if (ok) {
+      f = 0.0;
+      for (int i = 0; i < mm; ++i) f = fma(c[i], Fh[i * nn + t], f);
+      Ffull[t] = f;
+    }
+    Fin[t] = f;  // the matrix the next density is purified from
+  }
+  __syncthreads();
+}
+
+// Kernel feature bits (template FEAT): the tensor-core mixed form may be taken, DIIS is on.
+// Instances without a bit carry no call into its code (a call changes the register
+// allocation of the whole kernel).
+enum : int { FEAT_TENSOR = 1, FEAT_DIIS = 2 };
+
 template <int NT, int CR, int PLACE, int MX>
 __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
   const MolDesc d = a.mols[mi];
@@ -288,6 +403,14 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
     // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
     const bool purify = a.solver != SOLVER_JACOBI;
+    int diis_count = 0, diis_next = 0;
+    if constexpr ((MX & FEAT_DIIS) != 0) {
+      if (a.diis_depth >= 2) {  // F_in of the first step: the guess Fock matrix
+        double* Fin = diis_history(a, d.sq0) + 2 * (int64_t)a.diis_depth * n * n;
+        for (int t = threadIdx.x; t < n * n; t += blockDim.x) Fin[t] = Ffull[t];
+        __syncthreads();
+      }
+    }
     while (!conv && steps < a.max_iter) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {
@@ -301,7 +424,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
           Xr = Xo;
         } else {
           bool tensor = false;
-          if constexpr (MX == 1 && NT == 512) {
+          if constexpr ((MX & FEAT_TENSOR) && NT == 512) {
             // mixed form: TF32 tensor-core products (tcgen05), FP64 finish; X's region holds
             // the split copies (2 x max(128, n16) x n16 floats)
             const int n16 = purify_n16(n);
@@ -397,6 +520,10 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride + steps] = E;
       if (E != E) { status = MOL_NAN; break; }
       conv = fabs(Eold - E) < a.tol;
+      if constexpr ((MX & FEAT_DIIS) != 0) {
+        if (!conv && steps < a.max_iter && a.diis_depth >= 2 && status == MOL_OK)
+          block_diis<NT>(a, d.sq0, m, mi, Ffull, diis_count, diis_next, red);
+      }
     }
     if (purify && a.sorted_vectors && steps > 0 && status == MOL_OK) {
       // eigenpairs of the last F that produced a density (saved in m.V): one full Jacobi
@@ -456,9 +583,9 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
 }
 
 // NT threads per CTA; CR column registers per lane in the eigensolver (nao <= 32 * CR).
-// MX = 1: the instance that can take the tensor-core mixed form (launched only for that
-// solver); the FP64 instances carry no call into it, which would change their register
-// allocation.
+// MX: FEAT_* bits -- FEAT_TENSOR: the instance that can take the tensor-core mixed form
+// (launched only for that solver); FEAT_DIIS: the instance with DIIS (launched only with it
+// on).  The default instances (MX = 0) carry no call into either.
 template <int NT, int CR, int MX = 0>
 __global__ void __launch_bounds__(NT, 512 / NT) k_batch_scf(BatchArgs a) {
   extern __shared__ double smem[];

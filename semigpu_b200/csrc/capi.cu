@@ -125,6 +125,9 @@ struct sgb_batch {
   char* arena = nullptr;
   size_t bytes = 0;
   bool from_pool = false;
+  char* diis = nullptr;  // DIIS history (batched SCF with sgb_ctx_set_diis), on first use
+  size_t diis_bytes = 0;
+  int diis_depth = 0;
   MolDesc* d_desc = nullptr;
   int* d_order = nullptr;
   int* d_counter = nullptr;
@@ -396,6 +399,7 @@ void free_batch(sgb_batch* b) {
   } else if (b->arena) {
     arena_put(b->ctx, b->arena, b->bytes);
   }
+  if (b->diis) arena_put(b->ctx, b->diis, b->diis_bytes);
   give_event(b->ctx, b->ev0);
   give_event(b->ctx, b->ev1);
   delete b;
@@ -594,17 +598,26 @@ cudaError_t kernel_smem_cap(int* cap) {
   return cudaSuccess;
 }
 
+// The instances launch_feat<FEAT> can launch.
+template <int FEAT>
+cudaError_t prepare_feat(int* c) {
+  constexpr int D = FEAT & FEAT_DIIS;
+  cudaError_t e;
+  if ((e = kernel_smem_cap<512, 0, D>(c)) || (e = kernel_smem_cap<128, 2, D>(c)) ||
+      (e = kernel_smem_cap<256, 2, D>(c)) || (e = kernel_smem_cap<256, 3, D>(c)) ||
+      (e = kernel_smem_cap<256, 4, D>(c)) || (e = kernel_smem_cap<256, 5, D>(c)) ||
+      (e = kernel_smem_cap<512, 2, D>(c)) || (e = kernel_smem_cap<512, 3, FEAT>(c)) ||
+      (e = kernel_smem_cap<512, 4, FEAT>(c)) || (e = kernel_smem_cap<512, 5, FEAT>(c)))
+    return e;
+  return cudaSuccess;
+}
+
 // Every instantiation, at context creation (before any long launch can be running).
 cudaError_t prepare_kernels() {
   int c = 0;
   cudaError_t e;
-  if ((e = kernel_smem_cap<512, 0>(&c)) || (e = kernel_smem_cap<128, 2>(&c)) ||
-      (e = kernel_smem_cap<256, 2>(&c)) || (e = kernel_smem_cap<256, 3>(&c)) ||
-      (e = kernel_smem_cap<256, 4>(&c)) || (e = kernel_smem_cap<256, 5>(&c)) ||
-      (e = kernel_smem_cap<512, 2>(&c)) || (e = kernel_smem_cap<512, 3>(&c)) ||
-      (e = kernel_smem_cap<512, 4>(&c)) || (e = kernel_smem_cap<512, 5>(&c)) ||
-      (e = kernel_smem_cap<512, 3, 1>(&c)) || (e = kernel_smem_cap<512, 4, 1>(&c)) ||
-      (e = kernel_smem_cap<512, 5, 1>(&c)))
+  if ((e = prepare_feat<0>(&c)) || (e = prepare_feat<FEAT_TENSOR>(&c)) ||
+      (e = prepare_feat<FEAT_DIIS>(&c)) || (e = prepare_feat<FEAT_TENSOR | FEAT_DIIS>(&c)))
     return e;
   return cudaSuccess;
 }
@@ -625,31 +638,36 @@ cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStre
   return cudaGetLastError();
 }
 
-cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
-                         cudaStream_t st) {
-  if (cr == 0) return launch_kernel<512, 0>(num_sms, a, smem, st);
-  if (threads == 128 && cr == 2) return launch_kernel<128, 2>(num_sms, a, smem, st);
-  if (threads == 512 && a.solver == SOLVER_PURIFY_MIXED && cr >= 3) {  // tensor-core instances
-    switch (cr) {
-      case 3: return launch_kernel<512, 3, 1>(num_sms, a, smem, st);
-      case 4: return launch_kernel<512, 4, 1>(num_sms, a, smem, st);
-      default: return launch_kernel<512, 5, 1>(num_sms, a, smem, st);
-    }
-  }
+// FEAT_TENSOR only reaches the 512-thread classes of nao 65-160 (CR 3-5); FEAT_DIIS all.
+template <int FEAT>
+cudaError_t launch_feat(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
+                        cudaStream_t st) {
+  constexpr int D = FEAT & FEAT_DIIS;
+  if (cr == 0) return launch_kernel<512, 0, D>(num_sms, a, smem, st);
+  if (threads == 128 && cr == 2) return launch_kernel<128, 2, D>(num_sms, a, smem, st);
   if (threads == 512) {
     switch (cr) {
-      case 2: return launch_kernel<512, 2>(num_sms, a, smem, st);
-      case 3: return launch_kernel<512, 3>(num_sms, a, smem, st);
-      case 4: return launch_kernel<512, 4>(num_sms, a, smem, st);
-      default: return launch_kernel<512, 5>(num_sms, a, smem, st);
+      case 2: return launch_kernel<512, 2, D>(num_sms, a, smem, st);
+      case 3: return launch_kernel<512, 3, FEAT>(num_sms, a, smem, st);
+      case 4: return launch_kernel<512, 4, FEAT>(num_sms, a, smem, st);
+      default: return launch_kernel<512, 5, FEAT>(num_sms, a, smem, st);
     }
   }
   switch (cr) {
-    case 2: return launch_kernel<256, 2>(num_sms, a, smem, st);
-    case 3: return launch_kernel<256, 3>(num_sms, a, smem, st);
-    case 4: return launch_kernel<256, 4>(num_sms, a, smem, st);
-    default: return launch_kernel<256, 5>(num_sms, a, smem, st);
+    case 2: return launch_kernel<256, 2, D>(num_sms, a, smem, st);
+    case 3: return launch_kernel<256, 3, D>(num_sms, a, smem, st);
+    case 4: return launch_kernel<256, 4, D>(num_sms, a, smem, st);
+    default: return launch_kernel<256, 5, D>(num_sms, a, smem, st);
   }
+}
+
+cudaError_t launch_class(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
+                         cudaStream_t st) {
+  const bool tensor = a.solver == SOLVER_PURIFY_MIXED, diis = a.diis && a.diis_depth >= 2;
+  if (tensor && diis) return launch_feat<FEAT_TENSOR | FEAT_DIIS>(num_sms, a, cr, threads, smem, st);
+  if (tensor) return launch_feat<FEAT_TENSOR>(num_sms, a, cr, threads, smem, st);
+  if (diis) return launch_feat<FEAT_DIIS>(num_sms, a, cr, threads, smem, st);
+  return launch_feat<0>(num_sms, a, cr, threads, smem, st);
 }
 
 // Runs the requested stages over every molecule: one persistent launch per size class, each on
@@ -682,6 +700,23 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.t_begin = b->d_tb;
   a.t_end = b->d_te;
   a.stage_cycles = b->profiling ? b->d_stage : nullptr;
+  if (scf && ctx->diis >= 2) {
+    // history of depth F and residual matrices and the last F_in per molecule
+    // ((2 depth + 1) n^2) plus its B matrix
+    const size_t need =
+        8 * ((2 * (size_t)ctx->diis + 1) * (size_t)b->n_sq + (size_t)kDiisB * b->nmol);
+    if (b->diis && (b->diis_depth != ctx->diis || b->diis_bytes < need)) {
+      arena_put(ctx, b->diis, b->diis_bytes);
+      b->diis = nullptr;
+    }
+    if (!b->diis) {
+      if (int rc = arena_get(ctx, need, "DIIS history", &b->diis, &b->diis_bytes)) return rc;
+      b->diis_depth = ctx->diis;
+    }
+    a.diis = reinterpret_cast<double*>(b->diis);
+    a.diis_B = a.diis + (2 * (size_t)ctx->diis + 1) * (size_t)b->n_sq;
+    a.diis_depth = ctx->diis;
+  }
   cudaStream_t st = ctx->stream;
   CUDA_TRY(ctx, cudaMemsetAsync(b->d_counter, 0, sizeof(int) * kNumClasses, st));
   CUDA_TRY(ctx, cudaEventRecord(b->ev0, st));

@@ -181,3 +181,26 @@ def test_mixed_tensor_core_products_two_accumulators(gpu_ctx):
     assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
     np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
     assert np.all(np.abs(r["n_iter"] - ref["n_iter"]) <= 1)
+
+
+def test_batched_diis_same_energies_in_fewer_steps(gpu_ctx):
+    """Pulay DIIS in the batched launch (each CTA extrapolates its molecule's F): every molecule
+    converges to the energy of the reference's plain loop (within its tolerance) and the batch
+    needs fewer SCF steps; single molecules on one CTA take the same path."""
+    mols = geo.batch_c3(160, seed=31)
+    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ctx = sg.Context(0)
+    try:
+        ctx.set_diis(6)
+        r = sg.run_molecules(ctx, mols, tol=1e-6)
+        one = sg.Molecule.from_geometry(ctx, mols[7])
+        one.set_path(sg.PATH_CTA)
+        r1 = one.run(tol=1e-6)
+        one.close()
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-5)
+    assert r["n_iter"].sum() < ref["n_iter"].sum()
+    assert r1["converged"] and abs(r1["E_tot"] - ref["E_tot"][7]) < 1e-5
+    assert r1["n_iter"] == r["n_iter"][7]
