@@ -204,3 +204,21 @@ def test_batched_diis_same_energies_in_fewer_steps(gpu_ctx):
     assert r["n_iter"].sum() < ref["n_iter"].sum()
     assert r1["converged"] and abs(r1["E_tot"] - ref["E_tot"][7]) < 1e-5
     assert r1["n_iter"] == r["n_iter"][7]
+
+
+def test_mixed_precision_with_batched_diis(gpu_ctx):
+    """Both options at once (tensor-core products and DIIS in the same kernel instances):
+    converged, within the mixed form's 1e-4 eV of the plain FP64 loop."""
+    mols = geo.batch_c3(96, seed=41)
+    assert any(64 < m.nao <= 160 for m in mols)
+    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ctx = sg.Context(0)
+    try:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        ctx.set_diis(6)
+        r = sg.run_molecules(ctx, mols, tol=1e-6)
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
+    assert r["n_iter"].sum() < ref["n_iter"].sum()
