@@ -110,6 +110,11 @@ struct sgb_ctx {
   size_t staging_bytes = 0;
   cudaEvent_t staging_ev = nullptr;  // recorded after the last uploads read from it
   bool staging_busy = false;
+  // live batches and molecules of this context: sgb_ctx_destroy releases their device memory
+  // and detaches them, so destroying one afterwards (a garbage-collected wrapper) frees only
+  // its host part and never touches the freed context
+  std::vector<sgb_batch*> batches;
+  std::vector<sgb_mol*> mols;
 };
 
 struct sgb_batch {
@@ -394,6 +399,10 @@ cudaError_t download(sgb_ctx* ctx, const HostCopy* c, int n, cudaStream_t st) {
 
 void free_batch(sgb_batch* b) {
   if (!b) return;
+  if (b->ctx) {
+    auto& v = b->ctx->batches;
+    v.erase(std::remove(v.begin(), v.end(), b), v.end());
+  }
   if (b->arena && b->from_pool) {
     b->ctx->pool_busy = false;
   } else if (b->arena) {
@@ -560,6 +569,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     free_batch(b);
     return cuda_fail(ctx, e, "k_ang_to_bohr");
   }
+  ctx->batches.push_back(b);
   *out = b;
   return SGB_OK;
 }
@@ -1424,6 +1434,24 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
   cudaSetDevice(ctx->device);
   free_batch(ctx->cached);
   ctx->cached = nullptr;
+  // molecules and batches still alive: their device memory goes now, their host parts stay
+  // for their own destroy calls, which then no longer reach this context
+  for (sgb_mol* m : ctx->mols) {
+    free_grid_work(ctx, m);
+    m->ctx = nullptr;
+  }
+  ctx->mols.clear();
+  for (sgb_batch* b : ctx->batches) {
+    if (b->arena && !b->from_pool) arena_put(ctx, b->arena, b->bytes);
+    if (b->diis) arena_put(ctx, b->diis, b->diis_bytes);
+    give_event(ctx, b->ev0);
+    give_event(ctx, b->ev1);
+    b->arena = nullptr;
+    b->diis = nullptr;
+    b->ev0 = b->ev1 = nullptr;
+    b->ctx = nullptr;
+  }
+  ctx->batches.clear();
   if (ctx->pool) cudaFree(ctx->pool);
   {
     std::lock_guard<std::mutex> lock(ctx->spare_mutex);
@@ -1458,6 +1486,7 @@ int sgb_mol_create(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, sg
   if (rc) return rc;
   auto* m = new sgb_mol();
   m->ctx = ctx;
+  ctx->mols.push_back(m);
   m->b = b;
   *out = m;
   return SGB_OK;
@@ -1465,6 +1494,10 @@ int sgb_mol_create(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, sg
 
 int sgb_mol_destroy(sgb_mol* mol) {
   if (!mol) return SGB_E_ARG;
+  if (mol->ctx) {
+    auto& v = mol->ctx->mols;
+    v.erase(std::remove(v.begin(), v.end(), mol), v.end());
+  }
   free_grid_work(mol->ctx, mol);
   free_batch(mol->b);
   delete mol;

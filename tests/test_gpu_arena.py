@@ -78,3 +78,21 @@ def test_budget_reclaims_spare_arenas():
     finally:
         ctx.close()
     assert np.isfinite(e_small) and np.isfinite(e_big)
+
+
+def test_context_closed_before_its_molecules_and_batches():
+    """Closing a context first (a `with` block around objects collected later) releases their
+    device memory; destroying them afterwards touches only their host parts."""
+    ctx = sg.Context(0)
+    m = sg.Molecule.from_geometry(ctx, geo.ring_c1())
+    r = m.run(tol=1e-6)
+    b = sg.Batch(ctx, geo.batch_c3(8, seed=1))
+    b.run(1e-6)
+    b.results()
+    ctx.close()
+    m.close()
+    b.close()
+    assert r["converged"]
+    with sg.Context(0) as c2:
+        r2 = sg.run_molecules(c2, geo.batch_c3(4, seed=2), tol=1e-6)
+    assert np.all(r2["status"] == 0)
