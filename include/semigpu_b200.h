@@ -57,6 +57,9 @@ typedef struct {
 /* Binds a device, loads the MNDO tables, creates the stream.  hbm_budget_bytes = 0: no limit
  * beyond the device's own. */
 int sgb_ctx_create(int device, size_t hbm_budget_bytes, sgb_ctx **out);
+/* Frees the context's device and pinned host memory, streams and events.  Molecules and
+ * batches still alive lose their device memory here and stay valid only for their own destroy
+ * call (which then frees their host part alone). */
 int sgb_ctx_destroy(sgb_ctx *ctx);
 int sgb_ctx_synchronize(sgb_ctx *ctx);
 const char *sgb_last_error(const sgb_ctx *ctx);
