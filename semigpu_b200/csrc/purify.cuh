@@ -20,7 +20,7 @@
 //
 // Convergence: tr(X - X^2) = sum lambda (1 - lambda) is the idempotency error; once it is
 // below kPurifyIdem the eigenvalues are within ~1e-8 of 0 or 1 and kPurifyTail more steps
-// (quadratic) take them to rounding level.  A result is accepted only if tr(X) = nocc; a
+// (quadratic) take them to rounding level, unless it falls below kPurifyIdemFinal first.  A result is accepted only if tr(X) = nocc; a
 // vanishing HOMO-LUMO gap (no convergence within kPurifyMaxIter) or any non-finite value
 // reports failure, and the caller diagonalises instead.
 #pragma once
@@ -30,6 +30,10 @@ namespace sgb {
 
 constexpr int kPurifyMaxIter = 64;
 constexpr double kPurifyIdem = 1e-8;
+// Done at once when tr(X - X^2) is below this: every eigenvalue is then within 1e-11 of 0 or 1
+// (the tail after kPurifyIdem exists for the case where one side of the spectrum has not been
+// squared yet; reaching this bound first saves those products).
+constexpr double kPurifyIdemFinal = 1e-11;
 constexpr int kPurifyTail = 2;
 constexpr double kPurifyTraceTol = 1e-6;
 constexpr int kPurifyMaxN16 = 160;  // largest padded order held in one CTA's shared memory
@@ -381,6 +385,7 @@ __device__ int purify_fp64_loop(double* X, int n16, int ld, int nocc, double* re
   for (int it = it0; it <= kPurifyMaxIter; ++it) {
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) return -1;
     if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+    if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
     if (tail == 0) return fabs(t1 - (double)nocc) < kPurifyTraceTol ? it : -1;
     if (tail > 0) --tail;
     if (it == kPurifyMaxIter) break;
@@ -980,6 +985,7 @@ __device__ int block_purify_global(const double* F, int n, int nocc, double* X, 
   for (int it = 0; it <= kPurifyMaxIter; ++it) {
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) return -1;
     if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+    if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
     if (tail == 0) {
       *Xout = X;
       return fabs(t1 - (double)nocc) < kPurifyTraceTol ? it : -1;
