@@ -101,6 +101,26 @@ int sgb_ctx_set_sm_share(sgb_ctx *ctx, double share);
  * reference's; the converged energy is the same.  Next step after the reference's SCF loop
  * (scfcalculation.cpp:82-141), which has no convergence acceleration. */
 int sgb_ctx_set_diis(sgb_ctx *ctx, int depth);
+/* Density damping 0 <= factor < 1 (0 = off, the default) for every SCF of this context: the
+ * density that enters each Fock build is P = (1 - factor) P_new + factor P_previous.  Next step
+ * after the reference's SCF loop (scfcalculation.cpp:82-141), which takes P_new as is; it
+ * changes the SCF trajectory (damped oscillations), and the converged energy is the same. */
+int sgb_ctx_set_damping(sgb_ctx *ctx, double factor);
+/* Limits of the engine's bounded loops for this context (no counterpart in the reference,
+ * whose only bound is LAPACK's own, scfcalculation.cpp:87-93).  max_sweeps: Jacobi sweeps per
+ * eigensolve (0 = the default: 40 on one CTA, 60 on the grid path); an eigensolve that does not
+ * converge within it stops that molecule's SCF with SGB_E_EIG.  wait_spins: polls of each
+ * bounded device wait -- the first wait for a product's tensor-core MMAs (a timed-out wait
+ * abandons the purification of that SCF step, which is then diagonalised) and the grid-path
+ * barriers (a timed-out barrier ends the launch with SGB_E_CUDA); < 0 = the default bounds
+ * (hundreds of milliseconds to seconds).  Small values are for tests of those failure paths. */
+int sgb_ctx_set_limits(sgb_ctx *ctx, int max_sweeps, long long wait_spins);
+/* Failure-path check of the bounded grid barrier (no counterpart in the reference): launches
+ * `blocks` co-resident blocks (at most one per SM) at one barrier that expects blocks + extra
+ * arrivals; with extra > 0 it can never complete, so every block gives up after `spins` polls
+ * (>= 64 ns each) and the kernel ends.  *timed_out = 1 when the barrier reported its timeout. */
+int sgb_diag_barrier_timeout(sgb_ctx *ctx, int blocks, int extra, long long spins,
+                             int *timed_out);
 /* Reserves a reusable device arena of `bytes` for this context: a batch that fits is built in
  * it instead of allocating, and releasing the batch does not free device memory (cudaFree
  * synchronises the whole device, which would stall other contexts' work).  One batch at a time
@@ -233,9 +253,12 @@ int sgb_batch_device_coordinates(sgb_batch *b, void **dptr);
  * Limit: at most 128 atoms and 128 atomic orbitals (e.g. C32, C20H42); larger molecules are
  * rejected with SGB_E_UNSUPPORTED before any GPU work.  The first call on a device does that
  * device's set-up (loads the MNDO tables, looks up the scratch's device address), so it should
- * come before any stream capture.  Every call on a device uses the same scratch, which keeps the
- * previous call's contents: calls whose GPU work overlaps (other streams, other host threads)
- * race and must be serialised by the caller.  Returns SGB_OK, SGB_E_EIG, SGB_E_NAN, or an error. */
+ * come before any stream capture.  Each call is synchronous: it copies its inputs from host
+ * memory, and returns only after `stream` has finished the molecule and the results have been
+ * copied back.  Every call on a device uses the same scratch, which keeps the previous call's
+ * contents: calls whose GPU work overlaps (other streams, other host threads) race and must be
+ * serialised by the caller.  The solver follows SGB_DENSITY_SOLVER (see above).  Returns
+ * SGB_OK, SGB_E_EIG, SGB_E_NAN, or an error. */
 int sgb_scf_noalloc(int natoms, const int *Z, const double *xyz, double tol, int max_iter,
                     void *stream, double *e_el, double *e_cc, int *n_iter, int *converged,
                     int *status);

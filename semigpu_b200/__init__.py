@@ -43,6 +43,10 @@ SIGNATURES = {
     "sgb_ctx_set_density_solver": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_ctx_set_sm_share": (ctypes.c_int, [_VP, ctypes.c_double]),
     "sgb_ctx_set_diis": (ctypes.c_int, [_VP, ctypes.c_int]),
+    "sgb_ctx_set_damping": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "sgb_ctx_set_limits": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_longlong]),
+    "sgb_diag_barrier_timeout": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_longlong, _I]),
     "sgb_size_classes": (ctypes.c_int, [_I, _I, _I, ctypes.c_int]),
     "sgb_ctx_set_class_threads": (ctypes.c_int, [_VP, ctypes.c_int, _I]),
     "sgb_mndo_parameters": (ctypes.c_int, [ctypes.c_int, _D]),
@@ -173,6 +177,24 @@ class Context:
         """Pulay DIIS of this depth (2..8; 0 = off) for this context's SCF runs (batched
         launches and single molecules alike); step counts then differ from the reference's."""
         self.check(lib().sgb_ctx_set_diis(self.h, int(depth)), "set_diis")
+
+    def set_damping(self, factor: float):
+        """Density damping 0 <= factor < 1 (0 = off): P = (1 - f) P_new + f P_old each step."""
+        self.check(lib().sgb_ctx_set_damping(self.h, float(factor)), "set_damping")
+
+    def set_limits(self, max_sweeps: int = 0, wait_spins: int = -1):
+        """Jacobi sweeps per eigensolve (0 = default) and polls of each bounded device wait
+        (< 0 = default); small values exercise the failure paths."""
+        self.check(lib().sgb_ctx_set_limits(self.h, int(max_sweeps), int(wait_spins)),
+                   "set_limits")
+
+    def barrier_timeout_probe(self, blocks: int, extra: int, spins: int) -> bool:
+        """Launches a grid barrier that expects `extra` more blocks than it has; True when it
+        reported its timeout (see sgb_diag_barrier_timeout)."""
+        out = ctypes.c_int()
+        self.check(lib().sgb_diag_barrier_timeout(self.h, int(blocks), int(extra), int(spins),
+                                                  ctypes.byref(out)), "barrier probe")
+        return bool(out.value)
 
     def set_sm_share(self, share: float):
         """Batched launches of this context use at most this fraction of the SMs."""

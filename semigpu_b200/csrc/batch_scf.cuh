@@ -27,6 +27,8 @@
 
 namespace sgb {
 
+constexpr int kBatchJacobiSweeps = 40;
+
 struct BatchArgs {
   int nmol;
   const MolDesc* mols;
@@ -67,6 +69,15 @@ struct BatchArgs {
   double* diis = nullptr;
   double* diis_B = nullptr;
   int diis_depth = 0;
+  // Limits of the bounded loops: Jacobi sweeps per eigensolve (a non-converged eigensolve
+  // stops the molecule's SCF with MOL_EIG_FAILED, the reference's LAPACK info > 0 break), and
+  // polls of the first wait for a product's tensor-core MMAs (a timed-out wait abandons the
+  // purification of that step, which is then diagonalised).
+  int max_sweeps = kBatchJacobiSweeps;
+  long long wait_spins = kMbarSpins;
+  // Density damping (0 = off, the reference's plain loop): each step's density is mixed with
+  // the previous one, P = (1 - damping) P_new + damping P_old, before the Fock build.
+  double damping = 0.0;
 };
 
 // Stage timers (SM clock cycles of the CTA, thread 0, between block-wide barriers), the
@@ -186,7 +197,10 @@ __device__ __forceinline__ MolView make_view(const BatchArgs& a, const MolDesc& 
 
 // P (packed) = 2 Vo Vo^T with Vo = nocc column vectors (column-major, ldo) in shared memory;
 // 4x4 register tiles over the lower triangle of tiles.
-__device__ inline void block_density(int n, int nocc, const double* Vo, int ldo, double* P) {
+// With damping d > 0 the new density is mixed with the previous one still in P:
+// P = (1 - d) 2 Vo Vo^T + d P.
+__device__ inline void block_density(int n, int nocc, const double* Vo, int ldo, double* P,
+                                     double d) {
   const int tiles = (n + 3) >> 2;
   const int ntile = tiles * (tiles + 1) / 2;
   for (int t = threadIdx.x; t < ntile; t += blockDim.x) {
@@ -220,7 +234,10 @@ __device__ inline void block_density(int n, int nocc, const double* Vo, int ldo,
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int i = i0 + r, j = j0 + c;
-        if (i < n && j <= i) P[tri(i) + j] = 2.0 * acc[r][c];
+        if (i < n && j <= i) {
+          const double p = 2.0 * acc[r][c];
+          P[tri(i) + j] = d > 0.0 ? fma(d, P[tri(i) + j] - p, p) : p;
+        }
       }
   }
 }
@@ -401,6 +418,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
     E = block_fock_energy<NT>(m, Ffull, n, wq, Jc, stage, xs, hv, red);
     clk.lap(ST_FOCK);
     if (a.hist && threadIdx.x == 0) a.hist[(int64_t)mi * a.hist_stride] = E;
+    if (E != E) status = MOL_NAN;  // non-finite input (e.g. a NaN coordinate): no SCF step
     // purification needs X in shared memory (nao <= 160); larger molecules diagonalise
     const bool purify = a.solver != SOLVER_JACOBI;
     int diis_count = 0, diis_next = 0;
@@ -411,7 +429,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
         __syncthreads();
       }
     }
-    while (!conv && steps < a.max_iter) {
+    while (status == MOL_OK && !conv && steps < a.max_iter) {
       bool cold = steps == 0, jacobi = !purify;
       if (purify) {
         // ---- P from F by purification; a Jacobi eigensolve if that fails ----
@@ -430,14 +448,15 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
             const int n16 = purify_n16(n);
             tensor = a.solver == SOLVER_PURIFY_MIXED && n16 > 64 && n16 <= 160 &&
                      (size_t)(n16 > 128 ? n16 : 128) * n16 <= a.mat_doubles;
-            if (tensor) prod = block_purify_mixed<NT>(Ffull, n, m.nocc, smem, wq, red);
+            if (tensor)
+              prod = block_purify_mixed<NT>(Ffull, n, m.nocc, smem, wq, red, a.wait_spins);
           }
           if (!tensor) prod = block_purify<NT>(Ffull, n, m.nocc, smem, wq, red);
         }
         clk.lap(ST_PURIFY);
         clk.add(ST_PURIFY_PRODUCTS, (unsigned long long)(prod > 0 ? prod : 0));
         if (prod >= 0) {
-          purify_density(Xr, n, m.P);
+          purify_density(Xr, n, m.P, a.damping);
           __syncthreads();
           clk.lap(ST_DENSITY);
         } else {
@@ -467,7 +486,8 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
           split_by_rank(dval, n, nocc, occ, vir);
           __syncthreads();
           const bool o_small = nocc <= nvir;
-          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneGapped, 40,
+          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneGapped,
+                                       a.max_sweeps,
                                        o_small ? occ : vir, o_small ? nocc : nvir,
                                        o_small ? vir : occ, o_small ? nvir : nocc);
           if (sw >= 0) {
@@ -485,7 +505,8 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
         }
         if (full) {
           clk.add(ST_FULLJAC, 1);
-          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
+          sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs,
+                                       a.max_sweeps);
           if (sw >= 0) {
             block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);
             __syncthreads();
@@ -503,7 +524,7 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
           G[(int64_t)k * ld + i] = V[(int64_t)occ[k] * ldv + i];
         }
         __syncthreads();
-        block_density(n, m.nocc, G, ld, m.P);
+        block_density(n, m.nocc, G, ld, m.P, a.damping);
         __syncthreads();
         clk.lap(ST_DENSITY);
       }
@@ -539,7 +560,8 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
       __syncthreads();
       clk.start();
       clk.add(ST_FULLJAC, 1);
-      const int sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs, 40);
+      const int sw = block_jacobi_fv<NT, CR>(n, G, ld, V, ldv, red, kJacobiRotAbs, kJacobiDoneAbs,
+                                             a.max_sweeps);
       clk.add(ST_SWEEPS, (unsigned long long)(sw > 0 ? sw : 0));
       if (sw < 0) status = MOL_EIG_FAILED;
       else block_rayleigh<NT>(n, G, ld, V, ldv, 0.0, dval);

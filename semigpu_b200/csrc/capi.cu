@@ -86,6 +86,9 @@ struct sgb_ctx {
   int solver = SOLVER_PURIFY;  // SGB_SOLVER_*
   int sm_limit = 0;            // batched launches use at most this many SMs' worth of CTAs (0: all)
   int diis = 0;                // DIIS depth of the grid-path SCF (0: off)
+  int max_sweeps = 0;          // Jacobi sweeps per eigensolve (0: the path's default)
+  long long wait_spins = -1;   // polls of a bounded device wait (< 0: the default bound)
+  double damping = 0.0;        // density damping factor (0: off)
   cublasHandle_t blas = nullptr;  // created on first use (the products of grid purification)
   // Timing events for batches, created with the context and recycled: cudaEventCreate waits
   // for the kernels running on the device, which would stall a batch built while another
@@ -710,6 +713,9 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.t_begin = b->d_tb;
   a.t_end = b->d_te;
   a.stage_cycles = b->profiling ? b->d_stage : nullptr;
+  a.max_sweeps = ctx->max_sweeps > 0 ? ctx->max_sweeps : kBatchJacobiSweeps;
+  a.wait_spins = ctx->wait_spins >= 0 ? ctx->wait_spins : kMbarSpins;
+  a.damping = ctx->damping;
   if (scf && ctx->diis >= 2) {
     // history of depth F and residual matrices and the last F_in per molecule
     // ((2 depth + 1) n^2) plus its B matrix
@@ -766,6 +772,10 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
 constexpr int kGridThreads = 256;
 constexpr int kPartialMax = 4096;
 constexpr int kMaxSweeps = 60;
+
+long long barrier_spins(const sgb_ctx* ctx) {
+  return ctx->wait_spins >= 0 ? ctx->wait_spins : kBarrierSpins;
+}
 
 bool use_grid(const sgb_mol* mol) {
   if (mol->path == SGB_PATH_GRID) return true;
@@ -849,8 +859,10 @@ int grid_jacobi(sgb_ctx* ctx, sgb_mol* mol, const int* ga, int na, const int* gb
   GridJacobiArgs a;
   a.n = n; a.G = w.G; a.V = mol->b->d_V;
   a.grp_a = ga; a.na = na; a.grp_b = gb; a.nb = nb;
-  a.rot_abs = kJacobiRotAbs; a.done_abs = done_abs; a.max_sweeps = kMaxSweeps;
-  a.worst = w.worst; a.result = w.result; a.bar = GridBarrier{w.bar, w.bar + 1, w.err};
+  a.rot_abs = kJacobiRotAbs; a.done_abs = done_abs;
+  a.max_sweeps = ctx->max_sweeps > 0 ? std::min(ctx->max_sweeps, kMaxSweeps) : kMaxSweeps;
+  a.worst = w.worst; a.result = w.result;
+  a.bar = GridBarrier{w.bar, w.bar + 1, w.err, barrier_spins(ctx), 0u};
   int per_sm = 0;
   CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_jacobi, kGridThreads, 0));
   const int pairs = ga ? na : (n + 1) / 2;
@@ -975,7 +987,7 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
     if (tail < 0 && t[0] - t[1] < kPurifyIdem) tail = kPurifyTail;
     if (tail == 0) {
       if (fabs(t[0] - n_o) < kPurifyTraceTol) {
-        k_pur_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, X, v.P);
+        k_pur_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, X, v.P, ctx->damping);
         CUDA_TRY(ctx, cudaGetLastError());
         *products = it;
       }
@@ -1125,12 +1137,13 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   std::vector<double> hist(1, E);
   int steps = 0, conv = 0, status = SGB_OK;
+  if (E != E) status = SGB_E_NAN;  // non-finite input (e.g. a NaN coordinate): no SCF step
   const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
   const bool purify = ctx->solver != SOLVER_JACOBI;
   mol->eig_pending = false;
   DiisState ds;
   ds.depth = purify ? ctx->diis : 0;
-  while (!conv && steps < max_iter) {
+  while (status == SGB_OK && !conv && steps < max_iter) {
     const bool cold = steps == 0 || purify;
     bool have_p = false;  // P written by purification; a Jacobi eigensolve only if it failed
     if (purify) {
@@ -1174,7 +1187,7 @@ int scf_grid(sgb_ctx* ctx, sgb_mol* mol, double tol, int max_iter, sgb_scf_resul
       if (nocc > 0) {
         const int tiles = (n + 3) / 4;
         k_grid_density<<<grid_blocks(ctx, (int64_t)tiles * (tiles + 1) / 2), kGridThreads, 0, st>>>(
-            n, nocc, b->d_V, w.occ, v.P);
+            n, nocc, b->d_V, w.occ, v.P, ctx->damping);
       } else {
         CUDA_TRY(ctx, cudaMemsetAsync(v.P, 0, 8 * tri(n), st));
       }
@@ -1397,6 +1410,46 @@ int sgb_ctx_set_class_threads(sgb_ctx* ctx, int count, const int* threads) {
 int sgb_ctx_set_diis(sgb_ctx* ctx, int depth) {
   if (!ctx || depth < 0 || depth > 8 || depth == 1) return SGB_E_ARG;
   ctx->diis = depth;
+  return SGB_OK;
+}
+
+int sgb_ctx_set_damping(sgb_ctx* ctx, double factor) {
+  if (!ctx || !(factor >= 0.0 && factor < 1.0)) return SGB_E_ARG;
+  ctx->damping = factor;
+  return SGB_OK;
+}
+
+int sgb_ctx_set_limits(sgb_ctx* ctx, int max_sweeps, long long wait_spins) {
+  if (!ctx || max_sweeps < 0) return SGB_E_ARG;
+  ctx->max_sweeps = max_sweeps;
+  ctx->wait_spins = wait_spins < 0 ? -1 : wait_spins;
+  return SGB_OK;
+}
+
+int sgb_diag_barrier_timeout(sgb_ctx* ctx, int blocks, int extra, long long spins,
+                             int* timed_out) {
+  if (!ctx || blocks < 1 || extra < 0 || spins < 0 || !timed_out) return SGB_E_ARG;
+  if (blocks > ctx->num_sms) return fail(ctx, SGB_E_ARG, "at most %d blocks", ctx->num_sms);
+  char* mem = nullptr;
+  size_t got = 0;
+  if (int rc = arena_get(ctx, 256, "barrier probe", &mem, &got)) return rc;
+  cudaStream_t st = ctx->stream;
+  unsigned* bar = reinterpret_cast<unsigned*>(mem);
+  int* err = reinterpret_cast<int*>(mem + 16);
+  int h = 0;
+  cudaError_t e = cudaMemsetAsync(mem, 0, 32, st);
+  if (e == cudaSuccess) {
+    // one 32-thread block per SM at most, so every block is resident; a cooperative launch
+    // guarantees it
+    GridBarrier b{bar, bar + 1, err, spins, (unsigned)(blocks + extra)};
+    void* args[] = {&b};
+    e = cudaLaunchCooperativeKernel((void*)k_barrier_probe, blocks, 32, args, 0, st);
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, err, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  arena_put(ctx, mem, got);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "barrier probe");
+  *timed_out = h != 0;
   return SGB_OK;
 }
 

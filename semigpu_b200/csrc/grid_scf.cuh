@@ -11,13 +11,16 @@ namespace sgb {
 
 // ------------------------------------------------------------------------------------------
 // Grid barrier for a cooperative launch (all blocks co-resident).  Sense by generation count;
-// every wait is bounded: after kBarrierSpins polls the block records a timeout in *err and
-// returns false, and every block leaves at its next barrier.  With co-residency guaranteed by
-// the cooperative launch the bound is never reached in normal operation.
+// every wait is bounded: after `spins` polls the block records a timeout in *err and returns
+// false, and every block leaves at its next barrier.  With co-residency guaranteed by the
+// cooperative launch the bound is never reached in normal operation.  `expected` is the number
+// of arrivals that completes a barrier (0: the grid's block count).
 struct GridBarrier {
   unsigned* count;
   unsigned* gen;
   int* err;
+  long long spins;
+  unsigned expected;
 };
 
 constexpr long long kBarrierSpins = 1LL << 26;  // x >= 64 ns sleep: several seconds
@@ -29,14 +32,14 @@ __device__ bool grid_barrier(const GridBarrier& b) {
     const unsigned g = *vgen;
     __threadfence();
     const unsigned arrived = atomicAdd(b.count, 1u) + 1u;
-    if (arrived == gridDim.x) {
+    if (arrived == (b.expected ? b.expected : gridDim.x)) {
       *b.count = 0u;
       __threadfence();
       atomicAdd(b.gen, 1u);
     } else {
       long long spins = 0;
       while (*vgen == g) {
-        if (++spins > kBarrierSpins || *(volatile int*)b.err) {
+        if (++spins > b.spins || *(volatile int*)b.err) {
           atomicExch(b.err, 1);
           break;
         }
@@ -48,6 +51,11 @@ __device__ bool grid_barrier(const GridBarrier& b) {
   __syncthreads();
   return *(volatile int*)b.err == 0;
 }
+
+// One barrier expecting `expected` arrivals, for the wait-limit test: with more arrivals
+// expected than the grid has blocks, every block gives up after b.spins polls and *b.err is
+// set (no block waits longer than that).
+__global__ void k_barrier_probe(GridBarrier b) { grid_barrier(b); }
 
 __device__ __forceinline__ int64_t gtid() { return blockIdx.x * (int64_t)blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int64_t gstride() { return (int64_t)gridDim.x * blockDim.x; }
@@ -401,11 +409,13 @@ __global__ void k_lincomb(int64_t nn, LinComb lc, double* out) {
 }
 
 // P (packed lower triangle) = 2 X
-__global__ void k_pur_density(int n, const double* X, double* P) {
+// P = 2 X (packed), mixed with the previous P by the damping factor d when d > 0.
+__global__ void k_pur_density(int n, const double* X, double* P, double d) {
   for (int64_t t = gtid(); t < tri(n); t += gstride()) {
     int i, j;
     tri_inverse(t, i, j);
-    P[t] = 2.0 * X[(int64_t)i * n + j];
+    const double p = 2.0 * X[(int64_t)i * n + j];
+    P[t] = d > 0.0 ? fma(d, P[t] - p, p) : p;
   }
 }
 
@@ -504,8 +514,10 @@ __global__ void k_grid_crossing(int nocc, int nvir, const double* dval, const in
   }
 }
 
-// P (packed) = 2 sum_k V[:, occ[k]] V[:, occ[k]]^T, 4x4 register tiles on the lower triangle
-__global__ void k_grid_density(int n, int nocc, const double* V, const int* occ, double* P) {
+// P (packed) = 2 sum_k V[:, occ[k]] V[:, occ[k]]^T, 4x4 register tiles on the lower triangle;
+// mixed with the previous P by the damping factor d when d > 0
+__global__ void k_grid_density(int n, int nocc, const double* V, const int* occ, double* P,
+                               double d) {
   const int tiles = (n + 3) >> 2;
   const int64_t ntile = (int64_t)tiles * (tiles + 1) / 2;
   for (int64_t t = gtid(); t < ntile; t += gstride()) {
@@ -530,7 +542,10 @@ __global__ void k_grid_density(int n, int nocc, const double* V, const int* occ,
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int i = i0 + r, j = j0 + c;
-        if (i < n && j <= i) P[tri(i) + j] = 2.0 * acc[r][c];
+        if (i < n && j <= i) {
+          const double p = 2.0 * acc[r][c];
+          P[tri(i) + j] = d > 0.0 ? fma(d, P[tri(i) + j] - p, p) : p;
+        }
       }
   }
 }

@@ -450,7 +450,11 @@ __device__ __forceinline__ uint32_t umma_idesc_tf32(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-constexpr int kMbarSpins = 1 << 22;  // bounded wait for the MMAs (a few hundred ms at most)
+// Bounded wait for the MMAs of one product (x >= 64 ns sleep: a few hundred ms at most).  The
+// first wait of a product takes its bound from the caller (the context's wait limit, this value
+// by default); after a timed-out wait the second, recovery wait always uses this bound, so the
+// tensor memory is given back only after the MMAs that write it have completed.
+constexpr long long kMbarSpins = 1 << 22;
 // FP32 products until tr(X - X^2) falls below this (3xTF32 keeps X to ~1e-7, so the
 // idempotency error is still well above its FP32 floor of ~1e-5 here)
 constexpr double kPurifyTensorSwitch = 1e-4;
@@ -477,14 +481,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 template <int NT>
 __device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int nocc, double* X,
-                                                    double* lz, double* red);
+                                                    double* lz, double* red, long long spins);
 
 template <int NT>
 __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc, double* X,
-                                               double* lz, double* red) {
+                                               double* lz, double* red, long long spins) {
   constexpr int NW = NT / 32;
   static_assert(NT == 512, "the tensor-memory epilogue maps 16 warps onto 4 x 4 tiles of 32");
-  if (purify_n16(n) > 128) return block_purify_mixed_wide<NT>(F, n, nocc, X, lz, red);
+  if (purify_n16(n) > 128) return block_purify_mixed_wide<NT>(F, n, nocc, X, lz, red, spins);
   const int ld = purify_ld(n), n16 = purify_n16(n);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double t1, t2;
@@ -561,7 +565,7 @@ __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc,
           smem_u32(mbar)));
     }
     uint32_t done = 0;
-    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+    for (long long spin = 0; spin < spins && !done; ++spin) {
       asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                    "selp.u32 %0, 1, 0, p;\n\t}"
                    : "=r"(done)
@@ -724,7 +728,7 @@ __device__ __forceinline__ void wide_update(float* hi, float* lo, int n16, int r
 
 template <int NT>
 __device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int nocc, double* X,
-                                                    double* lz, double* red) {
+                                                    double* lz, double* red, long long spins) {
   constexpr int NW = NT / 32;
   static_assert(NT == 512, "the tensor-memory epilogue maps 16 warps onto 4 x 4 tiles of 32");
   const int ld = purify_ld(n), n16 = purify_n16(n), R = n16 - 128;  // R = 16 or 32
@@ -810,7 +814,7 @@ __device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int 
           smem_u32(mbar)));
     }
     uint32_t done = 0;
-    for (int spin = 0; spin < kMbarSpins && !done; ++spin) {
+    for (long long spin = 0; spin < spins && !done; ++spin) {
       asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                    "selp.u32 %0, 1, 0, p;\n\t}"
                    : "=r"(done)
@@ -1002,14 +1006,16 @@ __device__ int block_purify_global(const double* F, int n, int nocc, double* X, 
   return -1;
 }
 
-// P (packed lower triangle) = 2 X.
-__device__ inline void purify_density(const double* X, int n, double* P) {
+// P (packed lower triangle) = 2 X, or with density damping d > 0
+// P = (1 - d) 2 X + d P_previous (P holds the previous step's density on entry).
+__device__ inline void purify_density(const double* X, int n, double* P, double d) {
   const int ld = purify_ld(n);
   const int64_t np = tri(n);
   for (int64_t t = threadIdx.x; t < np; t += blockDim.x) {
     int i, j;
     tri_inverse(t, i, j);
-    P[t] = 2.0 * X[i * ld + j];
+    const double p = 2.0 * X[(int64_t)i * ld + j];
+    P[t] = d > 0.0 ? fma(d, P[t] - p, p) : p;
   }
 }
 

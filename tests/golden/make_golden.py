@@ -4,8 +4,12 @@ Run in a container that has the reference tree (it reads the reference's XYZ fix
 runs the reference); the fixtures it writes travel with the repository so the GPU-side tests
 never need the reference.
 
-    python tests/golden/make_golden.py            # everything except the long C100H202 run
-    python tests/golden/make_golden.py --c2       # add C100H202 (serial reference: ~2 h)
+    python tests/golden/make_golden.py --reference-src <reference>/src
+                                      # every fixture and synthetic case but C100H202
+    python tests/golden/make_golden.py --c2   # C100H202 alone (serial reference: ~2 h)
+
+The reference source tree is given by --reference-src or the SEMIGPU_REF_SRC environment
+variable (the directory holding common/, App/ and Geometries4Test/).
 
 Outputs (next to this script):
   reference_cases.json   per case: Z, xyz (Angstrom, as parsed by the reference reader), tol,
@@ -14,6 +18,9 @@ Outputs (next to this script):
   reference_matrices.npz element-level arrays for the small cases: integral blocks in the
                          reference's ragged [A][B<=A] order, Hcore, the guess P0 and its
                          Fock F0, the final P and F (packed lower triangles), eigenvalues.
+  reference_c100h202.npz (--c2) the all-trans C100H202 workload (302 atoms, 602 AOs, seed 0)
+                         at 1e-6 eV: geometry, per-step energies, step count, E_el / E_cc /
+                         E_tot, the final F and P (packed lower triangles) and eigenvalues.
 """
 from __future__ import annotations
 
@@ -35,8 +42,8 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 import oracle  # noqa: E402
 from semigpu_b200 import geometry as geo  # noqa: E402
 
-FIXTURE_DIR = "/root/reference/src/Geometries4Test"
 MATRIX_NAO_MAX = 40
+FIXTURE_DIR = None  # <reference>/src/Geometries4Test, set by main()
 
 
 def run_case(name, Z, xyz, tol, matrices, timeout=None):
@@ -60,7 +67,7 @@ def summarize(name, tol, r):
     return out
 
 
-def cases(with_c2: bool):
+def cases():
     out = []
     for path in sorted(glob.glob(os.path.join(FIXTURE_DIR, "*.xyz"))):
         base = os.path.basename(path)[:-4]
@@ -79,10 +86,25 @@ def cases(with_c2: bool):
                     ("polyene/C30H32", geo.polyene(30, rng)),
                     ("ring/C3H3N3", geo.aza_ring((0, 2, 4), rng))):
         out.append((name, m.Z, m.xyz, 1e-6, m.nao <= MATRIX_NAO_MAX))
-    if with_c2:
-        m = geo.alkane_c2(0)
-        out.append(("config/C100H202", m.Z, m.xyz, 1e-6, False))
     return out
+
+
+def c2_golden():
+    """C100H202 (the single-large-molecule workload) through the reference build, once."""
+    m = geo.alkane_c2(0)
+    t = time.time()
+    r = oracle.run_reference(m.Z, m.xyz, tol=1e-6, matrices=True)
+    wall = time.time() - t
+    print(f"C100H202 N={r['nao']} it={r['n_iter']} E_tot={r['E_tot']:.10f} {wall:.0f}s", flush=True)
+    np.savez_compressed(
+        os.path.join(HERE, "reference_c100h202.npz"),
+        Z=np.asarray(r["Z"], np.int32), xyz=np.asarray(r["xyz"], np.float64).reshape(-1, 3),
+        energies=np.asarray(r["energies"]), n_iter=np.int32(r["n_iter"]),
+        converged=np.bool_(r["converged"]), E_el=np.float64(r["E_el"]),
+        E_cc=np.float64(r["E_cc"]), E_tot=np.float64(r["E_tot"]),
+        F=np.asarray(r["F"], np.float64), P=np.asarray(r["P"], np.float64),
+        eig=np.asarray(r["eig"], np.float64), wall_s=np.float64(wall),
+        t_fock_s=np.float64(r["t_fock_s"]), t_eig_s=np.float64(r["t_eig_s"]))
 
 
 def readers():
@@ -118,16 +140,26 @@ def cli_outputs():
 
 
 def main():
+    global FIXTURE_DIR
     ap = argparse.ArgumentParser()
-    ap.add_argument("--c2", action="store_true")
+    ap.add_argument("--reference-src", default=os.environ.get("SEMIGPU_REF_SRC"),
+                    help="the reference's src/ directory (or set SEMIGPU_REF_SRC)")
+    ap.add_argument("--c2", action="store_true", help="only the C100H202 golden")
     ap.add_argument("--cli-only", action="store_true")
     ap.add_argument("--jobs", type=int, default=os.cpu_count())
     args = ap.parse_args()
+    if not args.reference_src:
+        ap.error("the reference source tree is required: --reference-src or SEMIGPU_REF_SRC")
+    FIXTURE_DIR = os.path.join(args.reference_src, "Geometries4Test")
+    os.environ["SEMIGPU_REF_SRC"] = args.reference_src
     oracle.build()
+    if args.c2:
+        c2_golden()
+        return
     cli_outputs()
     if args.cli_only:
         return
-    todo = cases(args.c2)
+    todo = cases()
     todo.sort(key=lambda c: -len(c[1]))
     summaries, mats = {}, {}
     with cf.ProcessPoolExecutor(args.jobs) as ex:

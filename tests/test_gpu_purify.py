@@ -114,7 +114,7 @@ def test_mixed_precision_within_tolerance(gpu_ctx, oracle_mod):
         ctx.close()
     o = oracle_mod.scf(mol.Z, mol.xyz, tol=1e-6)
     assert r["converged"] and r["status"] == 0
-    assert abs(r["E_tot"] - o["E_tot"]) <= 1e-4
+    assert abs(r["E_tot"] - o["E_tot"]) <= TOL_MIXED
     assert abs(r["n_iter"] - o["n_iter"]) <= 1
 
 
@@ -134,14 +134,24 @@ def test_diis_converges_to_the_same_energy_in_no_more_steps():
     assert abs(diis["E_tot"] - plain["E_tot"]) < 1e-5
 
 
-def test_mixed_tensor_core_products_in_batch(gpu_ctx):
-    """Mixed form in the batch: nao 65-128 (one 128-row tile) purify with TF32 tcgen05 products (3xTF32) and an FP64
-    finish; every molecule converges within 1e-4 eV of the FP64 form, without a fallback."""
+TOL_MIXED = 1e-4  # eV: |E_tot(mixed) - E_tot(FP64 oracle)| per molecule
+
+
+def _oracle_energies(oracle_mod, mols, tol=1e-6):
+    """E_tot and step counts of the FP64 oracle (the C restatement of the reference)."""
+    out = [oracle_mod.scf(m.Z, m.xyz, tol=tol) for m in mols]
+    return np.array([o["E_tot"] for o in out]), np.array([o["n_iter"] for o in out])
+
+
+def test_mixed_tensor_core_products_in_batch(gpu_ctx, oracle_mod):
+    """Mixed form in the batch: nao 65-128 (one 128-row tile) purify with TF32 tcgen05 products
+    (3xTF32) and an FP64 finish; every molecule converges within 1e-4 eV of the FP64 oracle,
+    without a fallback."""
     rng = np.random.default_rng(17)
     mols = [geo.alkane(k, rng) for k in (11, 13, 15, 17, 19, 21)]  # nao 68 .. 128
     mols += [geo.polyene(k, rng) for k in (14, 18, 22, 24)]           # nao 72 .. 122
     assert all(64 < m.nao <= 128 for m in mols)
-    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ref_e, _ = _oracle_energies(oracle_mod, mols)
     ctx = sg.Context(0)
     try:
         ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
@@ -155,17 +165,17 @@ def test_mixed_tensor_core_products_in_batch(gpu_ctx):
         ctx.close()
     assert np.all(r["status"] == 0) and np.all(r["converged"])
     assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
-    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
+    np.testing.assert_allclose(r["E_tot"], ref_e, rtol=0, atol=TOL_MIXED)
 
 
-def test_mixed_tensor_core_products_two_accumulators(gpu_ctx):
+def test_mixed_tensor_core_products_two_accumulators(gpu_ctx, oracle_mod):
     """nao 129-160 (n16 144 and 160): X taller than one 128-row tile, products from two
     tensor-memory accumulators plus symmetry; same bar as the single-tile form."""
     rng = np.random.default_rng(23)
     mols = [geo.alkane(k, rng) for k in (22, 23, 24, 25, 26)]  # nao 134 .. 158
     mols += [geo.polyene(k, rng) for k in (26, 28, 30)]         # nao 132 .. 152
     assert {(m.nao + 15) // 16 * 16 for m in mols} == {144, 160}
-    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ref_e, ref_it = _oracle_energies(oracle_mod, mols)
     ctx = sg.Context(0)
     try:
         ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
@@ -179,8 +189,8 @@ def test_mixed_tensor_core_products_two_accumulators(gpu_ctx):
         ctx.close()
     assert np.all(r["status"] == 0) and np.all(r["converged"])
     assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
-    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
-    assert np.all(np.abs(r["n_iter"] - ref["n_iter"]) <= 1)
+    np.testing.assert_allclose(r["E_tot"], ref_e, rtol=0, atol=TOL_MIXED)
+    assert np.all(np.abs(r["n_iter"] - ref_it) <= 1)
 
 
 def test_batched_diis_same_energies_in_fewer_steps(gpu_ctx):
@@ -206,12 +216,13 @@ def test_batched_diis_same_energies_in_fewer_steps(gpu_ctx):
     assert r1["n_iter"] == r["n_iter"][7]
 
 
-def test_mixed_precision_with_batched_diis(gpu_ctx):
+def test_mixed_precision_with_batched_diis(gpu_ctx, oracle_mod):
     """Both options at once (tensor-core products and DIIS in the same kernel instances):
-    converged, within the mixed form's 1e-4 eV of the plain FP64 loop."""
+    converged, within the mixed form's 1e-4 eV of the FP64 oracle's plain loop."""
     mols = geo.batch_c3(96, seed=41)
     assert any(64 < m.nao <= 160 for m in mols)
     ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    ref_e, _ = _oracle_energies(oracle_mod, mols)
     ctx = sg.Context(0)
     try:
         ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
@@ -220,5 +231,22 @@ def test_mixed_precision_with_batched_diis(gpu_ctx):
     finally:
         ctx.close()
     assert np.all(r["status"] == 0) and np.all(r["converged"])
-    np.testing.assert_allclose(r["E_tot"], ref["E_tot"], rtol=0, atol=1e-4)
+    np.testing.assert_allclose(r["E_tot"], ref_e, rtol=0, atol=TOL_MIXED)
     assert r["n_iter"].sum() < ref["n_iter"].sum()
+
+
+def test_mixed_batch_composition_against_oracle(oracle_mod):
+    """The bench batch's composition (every size class) in the mixed form: each molecule's
+    E_tot within 1e-4 eV of the FP64 oracle, the error reported per molecule."""
+    mols = geo.batch_c3(256, seed=0)
+    ref_e, ref_it = _oracle_energies(oracle_mod, mols)
+    ctx = sg.Context(0)
+    try:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        r = sg.run_molecules(ctx, mols, tol=1e-6)
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    err = np.abs(r["E_tot"] - ref_e)
+    assert err.max() <= TOL_MIXED, (int(err.argmax()), float(err.max()))
+    assert np.all(np.abs(r["n_iter"] - ref_it) <= 1)
