@@ -2,6 +2,9 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+With --gpus N > 1 and no torchrun around it, bench.py starts N ranks of itself under
+torch.distributed.run; under torchrun, WORLD_SIZE must equal N.
+
 A step is one persistent launch that takes every molecule of the batch from coordinates to
 converged total energy (integrals, Hcore, SCF, core-core).  `value` is device-timed
 (CUDA events recorded by the library around each launch, inputs resident in HBM);
@@ -50,12 +53,14 @@ def env_int(name, default):
 # Clock sampling during the timed region
 
 class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons of the given GPUs (every rank's
+    GPU when rank 0 samples for the job), every 200 ms while the timed region runs."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
-        self.device = device
+    def __init__(self, devices):
+        self.devices = [devices] if isinstance(devices, int) else list(devices)
         self.proc = None
         self.path = None
 
@@ -64,7 +69,8 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                ["nvidia-smi", "-i", ",".join(str(d) for d in self.devices),
+                 f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
@@ -105,7 +111,7 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "gpus": sorted({r[0] for r in rows})}
 
 
 # ------------------------------------------------------------------------------------------
@@ -164,23 +170,72 @@ def stratified(mols, k, offset=0):
 
 
 def _ref_one(args):
+    """One molecule through the reference build (single-threaded process, OpenBLAS on one
+    thread); returns E_tot, steps, CPU-seconds and wall seconds of that process."""
+    import resource
+
     Z, xyz = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
+    c0 = resource.getrusage(resource.RUSAGE_CHILDREN)
+    t0 = time.perf_counter()
     r = oracle.run_reference(Z, xyz, tol=TOL, matrices=False)
-    return r["E_tot"], r["n_iter"]
+    wall = time.perf_counter() - t0
+    c1 = resource.getrusage(resource.RUSAGE_CHILDREN)
+    cpu = (c1.ru_utime + c1.ru_stime) - (c0.ru_utime + c0.ru_stime)
+    return r["E_tot"], r["n_iter"], cpu, wall
 
 
-def time_reference(sample, cores):
-    """Wall time of the reference CLI engine over `sample`, one molecule per process."""
+def _pool_ready(_):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle  # noqa: F401
+
+    return os.getpid()
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_queue(sample, cores):
+    """The reference build over `sample` as a work queue: one single-threaded reference process
+    per core, molecules handed out longest first (the sample is ordered by decreasing nao, the
+    cost being ~nao^4 per Fock build), each core taking the next molecule as soon as it is
+    free.  The pool is started before the timed region.  Returns wall seconds, the summed
+    CPU-seconds of the reference processes and the per-molecule results."""
     import multiprocessing as mp
 
     ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(min(cores, len(sample))) as pool:
-        out = pool.map(_ref_one, [(m.Z, m.xyz) for m in sample], chunksize=1)
-    return time.perf_counter() - t0, out
+    workers = min(cores, len(sample))
+    with ctx.Pool(workers) as pool:
+        pool.map(_pool_ready, range(workers), chunksize=1)
+        t0 = time.perf_counter()
+        out = list(pool.imap(_ref_one, [(m.Z, m.xyz) for m in sample], chunksize=1))
+        wall = time.perf_counter() - t0
+    return wall, sum(o[2] for o in out), out
+
+
+def cpu_baseline_record(sample, cores, wall, cpu_s, label):
+    """The cpu_baseline object: whole-queue throughput on `cores` cores, with the CPU-seconds
+    per molecule, the cores' busy fraction and the serial (one core) throughput beside it."""
+    n = len(sample)
+    return {"value": n / wall, "unit": UNIT, "cores": min(cores, n), "kind": "reference",
+            "cpu_model": cpu_model(), "host_cores": os.cpu_count(),
+            "cpu_s_per_molecule": cpu_s / n, "wall_s": wall,
+            "utilization": cpu_s / (wall * min(cores, n)),
+            "serial_1core": {"value": n / cpu_s, "unit": UNIT,
+                             "how": "molecules / summed CPU-seconds of the single-threaded "
+                                    "reference processes (OPENBLAS_NUM_THREADS=1)"},
+            "sample": f"{n} molecules of {label}, stratified by nao, one work queue "
+                      f"(longest first) over {min(cores, n)} single-threaded reference processes"}
 
 
 def reference_kind():
@@ -205,27 +260,25 @@ def run_reference_arm(args):
         return
     mols = geo.batch_c3(BATCH, seed=0)
     cores = os.cpu_count() or 1
-    per_step = max(cores, 8)
-    times, done = [], 0
+    # one stratified sample of ~256 molecules (at least one per core and step), run as a single
+    # work queue across the K timed steps so the cores stay busy; warm-up: a few small ones
+    per_step = max(cores, -(-256 // max(1, args.steps)))
+    sample = stratified(mols, per_step * args.steps)
     small = sorted(mols, key=lambda m: m.nao)[: len(mols) // 4]
-    for s in range(args.warmup + args.steps):
-        # warm-up steps run a light sample (process-pool start-up, page cache)
-        sample = stratified(small if s < args.warmup else mols, per_step, offset=s)
-        dt, _ = time_reference(sample, cores)
-        if s >= args.warmup:
-            times.append(dt)
-            done += len(sample)
-    total = sum(times)
-    value = done / total
+    if args.warmup:
+        reference_queue(stratified(small, max(1, min(cores, 2 * args.warmup))), cores)
+    wall, cpu_s, _ = reference_queue(sample, cores)
+    value = len(sample) / wall
+    cpu = cpu_baseline_record(sample, cores, wall, cpu_s, "the seed-0 4096-molecule batch")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
         "config": {"workload": WORKLOAD, "sample_per_step": per_step,
-                   "sample": "stratified by nao over the seed-0 batch, shifted each step"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{per_step} molecules per step, stratified by nao"},
+                   "sample": f"{len(sample)} molecules stratified by nao over the seed-0 batch, "
+                             f"one work queue over the {args.steps} steps"},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -274,7 +327,7 @@ def run_ours(args):
     barrier()
     kernel_ms = []
     lat_p50, lat_p99 = [], []
-    with ClockSampler(local) as clocks:
+    with ClockSampler(list(range(world)) if rank == 0 else [local]) as clocks:
         for _ in range(args.steps):
             flush.fill_(1.0)
             torch.cuda.synchronize(dev)
@@ -440,12 +493,9 @@ def run_ours(args):
         cpu = None
         if reference_kind():
             cores = os.cpu_count() or 1
-            csample = stratified(mols, max(16, min(cores, 32)))
-            dt, _ = time_reference(csample, cores)
-            cpu = {"value": len(csample) / dt, "unit": UNIT, "cores": min(cores, len(csample)),
-                   "kind": "reference",
-                   "sample": f"{len(csample)} molecules stratified by nao from the same batch, "
-                             f"one reference process per molecule ({dt:.1f} s wall)"}
+            csample = stratified(mols, max(cores, 160))
+            dt, cpu_s, _ = reference_queue(csample, cores)
+            cpu = cpu_baseline_record(csample, cores, dt, cpu_s, "the same batch")
         nat_total = int(natoms.sum())
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -501,11 +551,49 @@ def main():
     ap.add_argument("--kernel-only", action="store_true",
                     help="device-timed launches only (no e2e, plain-path or CPU legs); used "
                          "for profiler captures of a smaller batch")
+    ap.add_argument("--probe-ranks", action="store_true",
+                    help="print this process's rank and world size as JSON and exit (no GPU "
+                         "work): shows how `--gpus N` lays out its processes")
     args = ap.parse_args()
+    if args.gpus < 1:
+        ap.error("--gpus must be >= 1")
+    rc = launch_ranks(args)
+    if rc is not None:
+        sys.exit(rc)
+    if args.probe_ranks:
+        print(json.dumps({"rank": env_int("RANK", 0), "world": env_int("WORLD_SIZE", 1),
+                          "local_rank": env_int("LOCAL_RANK", 0), "gpus": args.gpus}), flush=True)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
     else:
         run_ours(args)
+
+
+def _free_port() -> int:
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_ranks(args):
+    """One process per GPU.  Under torchrun (WORLD_SIZE set) the world must be --gpus and this
+    process carries on (None); launched plainly with --gpus N > 1, bench.py starts N ranks of
+    itself under torch.distributed.run on 127.0.0.1 and returns their exit status."""
+    world = os.environ.get("WORLD_SIZE")
+    if world is not None:
+        if int(world) != args.gpus:
+            print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}", file=sys.stderr)
+            return 2
+        return None
+    if args.gpus == 1:
+        return None
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr=127.0.0.1",
+           f"--master-port={_free_port()}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.run(cmd).returncode
 
 
 if __name__ == "__main__":

@@ -196,6 +196,11 @@ int sgb_core_core(sgb_ctx *ctx, sgb_mol *mol, double *e_cc);
  * ElectronicEnergy::ComputeEnergy (electronicenergy.cpp:12-36) for a caller-given packed
  * density P: F = Hcore + G(P) into F (packed, host), E_el into *e_el (may be NULL). */
 int sgb_fock(sgb_ctx *ctx, sgb_mol *mol, const double *P, double *F, double *e_el);
+/* Replaces ElectronicEnergy::ComputeEnergy (electronicenergy.cpp:12-36): E_el =
+ * 1/2 sum_ij P_ij (H_ij + F_ij) over caller-given packed nao x nao matrices, reduced on the
+ * device in a fixed order. */
+int sgb_electronic_energy(sgb_ctx *ctx, int nao, const double *H, const double *F,
+                          const double *P, double *e_el);
 /* Copies one of SGB_BLOCKS .. SGB_EIGVEC to host memory (sizes: see sgb_mol_info; packed
  * matrices nao*(nao+1)/2, SGB_EIGVAL nao, SGB_EIGVEC nao*nao).  Replaces reading
  * TwoCenterIntegral::GetValueFromArray / BaseMatrix::matrixHold_ / SCFCalculation::eigenVec. */

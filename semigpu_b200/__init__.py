@@ -61,6 +61,7 @@ SIGNATURES = {
     "sgb_core_core": (ctypes.c_int, [_VP, _VP, _D]),
     "sgb_fock": (ctypes.c_int, [_VP, _VP, _D, _D, _D]),
     "sgb_get": (ctypes.c_int, [_VP, _VP, ctypes.c_int, _D, ctypes.c_size_t]),
+    "sgb_electronic_energy": (ctypes.c_int, [_VP, ctypes.c_int, _D, _D, _D, _D]),
     "sgb_batch_create": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.POINTER(_VP)]),
     "sgb_batch_destroy": (ctypes.c_int, [_VP]),
     "sgb_batch_set_coordinates": (ctypes.c_int, [_VP, _VP, _D]),
@@ -177,6 +178,18 @@ class Context:
         """Pulay DIIS of this depth (2..8; 0 = off) for this context's SCF runs (batched
         launches and single molecules alike); step counts then differ from the reference's."""
         self.check(lib().sgb_ctx_set_diis(self.h, int(depth)), "set_diis")
+
+    def electronic_energy(self, H, F, P) -> float:
+        """E_el = 1/2 sum P (H + F) of packed matrices (ElectronicEnergy::ComputeEnergy),
+        reduced on the device."""
+        H, F, P = (np.ascontiguousarray(x, np.float64) for x in (H, F, P))
+        n = int((np.sqrt(8 * len(H) + 1) - 1) / 2)
+        if not (len(H) == len(F) == len(P) == n * (n + 1) // 2):
+            raise ValueError("H, F, P must be packed triangles of one order")
+        e = ctypes.c_double()
+        self.check(lib().sgb_electronic_energy(self.h, n, _d(H), _d(F), _d(P), ctypes.byref(e)),
+                   "sgb_electronic_energy")
+        return e.value
 
     def set_damping(self, factor: float):
         """Density damping 0 <= factor < 1 (0 = off): P = (1 - f) P_new + f P_old each step."""

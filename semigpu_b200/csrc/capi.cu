@@ -1679,6 +1679,36 @@ int sgb_fock(sgb_ctx* ctx, sgb_mol* mol, const double* P, double* F, double* e_e
   return sgb_ctx_synchronize(ctx);
 }
 
+int sgb_electronic_energy(sgb_ctx* ctx, int nao, const double* H, const double* F,
+                          const double* P, double* e_el) {
+  if (!ctx || nao <= 0 || !H || !F || !P || !e_el) return SGB_E_ARG;
+  const int64_t np = tri(nao);
+  const int nb = grid_blocks(ctx, np);
+  const size_t mat = align_up(8 * (size_t)np);
+  char* mem = nullptr;
+  size_t got = 0;
+  if (int rc = arena_get(ctx, 3 * mat + 8 * (size_t)(nb + 1), "energy inputs", &mem, &got))
+    return rc;
+  double* dH = reinterpret_cast<double*>(mem);
+  double* dF = reinterpret_cast<double*>(mem + mat);
+  double* dP = reinterpret_cast<double*>(mem + 2 * mat);
+  double* part = reinterpret_cast<double*>(mem + 3 * mat);
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(dH, H, 8 * np, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dF, F, 8 * np, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dP, P, 8 * np, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    k_energy_partials<<<nb, kGridThreads, 0, st>>>(np, dH, dF, dP, part);
+    k_reduce_sum<<<1, 256, 0, st>>>(part, nb, part + nb);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(e_el, part + nb, 8, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  arena_put(ctx, mem, got);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "electronic energy");
+  return SGB_OK;
+}
+
 int sgb_get(sgb_ctx* ctx, const sgb_mol* mol, int which, double* host, size_t count) {
   if (!ctx || !mol || !host) return SGB_E_ARG;
   if ((which == SGB_EIGVAL || which == SGB_EIGVEC) && mol->eig_pending) {

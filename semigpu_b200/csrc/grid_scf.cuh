@@ -160,6 +160,22 @@ __global__ void k_reduce_sum(const double* partial, int n, double* out) {
   }
 }
 
+// E_el = 1/2 sum_ij P_ij (H_ij + F_ij) over the full symmetric matrices from their packed lower
+// triangles (electronicenergy.cpp:12-36: the triangle twice, the diagonal once): block partials
+// of (H + F) P weighted 1 off the diagonal and 1/2 on it; k_reduce_sum finishes the sum.
+__global__ void k_energy_partials(int64_t np, const double* __restrict__ H,
+                                  const double* __restrict__ F, const double* __restrict__ P,
+                                  double* partial) {
+  double e = 0.0;
+  for (int64_t t = gtid(); t < np; t += gstride()) {
+    int i, j;
+    tri_inverse(t, i, j);
+    const double v = (H[t] + F[t]) * P[t];
+    e += i == j ? 0.5 * v : v;
+  }
+  write_block_partial(e, partial);
+}
+
 // ------------------------------------------------------------------------------------------
 // Purification on the whole GPU: the recursion of purify.cuh for one large molecule.  The
 // products X^2 are symmetric rank-n updates issued by the host loop (cuBLAS DSYRK, lower

@@ -370,6 +370,19 @@ void FockMatrix::ComputeMatrix() {
         "sgb_fock");
 }
 
+// ---- ElectronicEnergy -------------------------------------------------------------------------
+ElectronicEnergy::ElectronicEnergy() {}
+
+double ElectronicEnergy::ComputeEnergy(const size_t& nAOs, const Hcore& hcore,
+                                       const FockMatrix& Fmatrix, const DensityMatrix& Pmatrix) {
+  if (!hcore.matrixHold_ || !Fmatrix.matrixHold_ || !Pmatrix.matrixHold_ || nAOs == 0) return 0.0;
+  double e = 0.0;
+  check(sgb_electronic_energy(semigpu::context(), (int)nAOs, hcore.matrixHold_,
+                              Fmatrix.matrixHold_, Pmatrix.matrixHold_, &e),
+        "sgb_electronic_energy");
+  return e;
+}
+
 // ---- SCFCalculation ---------------------------------------------------------------------------
 SCFCalculation::SCFCalculation(const ListAtomicOrbitals& infoAOs, double****& ints, const Hcore& h)
     : eigenVec(nullptr), eigenVal(nullptr), Pmatrix(nullptr), Fmatrix(nullptr), finalEnergy(0.0),

@@ -159,6 +159,16 @@ class FockMatrix : public BaseMatrix {
   const DensityMatrix* Pmatrix_;
 };
 
+// ---- electronicenergy.h -----------------------------------------------------------------
+class ElectronicEnergy {
+ public:
+  ElectronicEnergy();
+  // 1/2 sum_ij P_ij (H_ij + F_ij) of the three matrixHold_ arrays (electronicenergy.cpp:12-36),
+  // reduced on the device
+  static double ComputeEnergy(const size_t& nAOs, const Hcore&, const FockMatrix&,
+                              const DensityMatrix&);
+};
+
 // ---- scfcalculation.h -------------------------------------------------------------------
 class SCFCalculation {
  public:
