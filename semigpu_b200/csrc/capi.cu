@@ -15,6 +15,7 @@
 
 #include "../../include/semigpu_b200.h"
 #include "batch_scf.cuh"
+#include "grid_purify.cuh"
 #include "grid_scf.cuh"
 #include "layout.h"
 #include "mndo_tables.cuh"
@@ -164,7 +165,9 @@ struct GridWork {
   char* arena = nullptr;
   size_t bytes = 0;
   double *G = nullptr, *Fprev = nullptr, *wq = nullptr, *dval = nullptr, *partial = nullptr;
-  double* X2 = nullptr;  // purification product (G holds X)
+  double* X2 = nullptr;  // purification: X and its partner are G and X2 (padded order xnp)
+  int xbuf = 0;          // which of G (0) / X2 (1) holds the last purified X
+  int xnp = 0;           // its padded order
   unsigned* count = nullptr;  // last-block counter of the fused reductions (0 between uses)
   // DIIS history (grid path, when enabled): depth x (F, error) n x n pairs, and the B matrix
   double* diis = nullptr;
@@ -798,16 +801,21 @@ int grid_blocks(const sgb_ctx* ctx, int64_t tasks) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, std::min<int64_t>(kPartialMax, 8LL * ctx->num_sms)));
 }
 
+// Padded order of the purification buffers: a multiple of the largest tile (128), so every
+// tile configuration fits the same allocation.
+int64_t grid_pad(int64_t n) { return (n + GpLarge::BM - 1) / GpLarge::BM * GpLarge::BM; }
+
 int ensure_grid_work(sgb_ctx* ctx, sgb_mol* mol) {
   GridWork& w = mol->gw;
   if (w.arena) return SGB_OK;
   const int64_t n = mol->b->desc[0].nao;
+  const int64_t np = grid_pad(n);  // X and its partner: padded to the largest purify tile
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off = align_up(off + bytes); return o; };
-  const size_t oG = take(8 * n * n), oFp = take(8 * n * n), oX2 = take(8 * n * n),
+  const size_t oG = take(8 * np * np), oFp = take(8 * n * n), oX2 = take(8 * np * np),
                owq = take(8 * (3 * n + 8)), odv = take(8 * n), opart = take(8 * 2 * kPartialMax),
                osc = take(8 * 16),
-               oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(4),
+               oocc = take(4 * n), ovir = take(4 * n), oflag = take(4), ores = take(16),
                ocount = take(8),
                owst = take(8 * kMaxSweeps), obar = take(8), oerr = take(4);
   if (int rc = arena_get(ctx, off, "grid workspace", &w.arena, &w.bytes)) return rc;
@@ -923,25 +931,102 @@ int grid_lanczos_bounds(sgb_ctx* ctx, sgb_mol* mol, double* lohi) {
   return SGB_OK;
 }
 
+// Tile configuration of the device purification loop for order n: the largest tile that
+// still gives every SM work (two tiles per SM for the 128 x 128 tile, one for 64 x 64).
+int gp_tile(int n, int num_sms) {
+  auto tiles = [](int n, int bm) { const int64_t t = (n + bm - 1) / bm; return t * (t + 1) / 2; };
+  if (tiles(n, GpLarge::BM) >= 2LL * num_sms) return GpLarge::BM;
+  if (tiles(n, GpMid::BM) >= num_sms) return GpMid::BM;
+  return GpSmall::BM;
+}
+
+// Dynamic shared memory cap of each configuration, once per device (cudaFuncSetAttribute
+// waits for running kernels, so this runs at context creation).
+template <class C>
+cudaError_t gp_prepare() {
+  static bool done[kMaxDevices] = {};
+  static std::mutex m;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(m);
+  if (!done[dev]) {
+    e = cudaFuncSetAttribute(k_grid_purify<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)C::SMEM);
+    if (e != cudaSuccess) return e;
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t prepare_grid_purify() {
+  cudaError_t e;
+  if ((e = gp_prepare<GpLarge>()) || (e = gp_prepare<GpMid>()) || (e = gp_prepare<GpSmall>()))
+    return e;
+  return cudaSuccess;
+}
+
+// One cooperative launch of the device purification loop on X_0 in buffer 0 (padded order
+// np, sums at t0); *products and *xbuf from its result.
+template <class C>
+int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, int* products, int* xbuf) {
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  const int nocc = mol->b->desc[0].nocc;
+  CUtensorMap maps[2];
+  double* bufs[2] = {w.G, w.X2};
+  for (int k = 0; k < 2; ++k)
+    if (!make_tensor_map_2d(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, bufs[k], np, np, np,
+                            C::BM, kGpK))
+      return fail(ctx, SGB_E_CUDA, "tensor map of the purification buffers (np = %d)", np);
+  CUDA_TRY(ctx, gp_prepare<C>());
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_purify<C>,
+                                                              C::THREADS, C::SMEM));
+  if (per_sm < 1) return fail(ctx, SGB_E_CUDA, "purification kernel does not fit an SM");
+  const int nt = np / C::BM;
+  const int grid = (int)std::min<int64_t>((int64_t)nt * (nt + 1) / 2,
+                                          std::min<int64_t>((int64_t)per_sm * ctx->num_sms,
+                                                            kPartialMax / 4));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.bar, 0, 8, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.err, 0, 4, st));
+  GridPurifyArgs a;
+  a.np = np;
+  a.nocc = nocc;
+  a.buf[0] = bufs[0];
+  a.buf[1] = bufs[1];
+  a.partial = w.partial;
+  a.t0 = w.scalars + 4;
+  a.result = w.result;
+  a.bar = GridBarrier{w.bar, w.bar + 1, w.err, barrier_spins(ctx), 0u};
+  a.spins = ctx->wait_spins >= 0 ? ctx->wait_spins : kMbarSpins;
+  a.it0 = it0;
+  void* args[] = {&maps[0], &maps[1], &a};
+  CUDA_TRY(ctx, cudaLaunchCooperativeKernel((void*)k_grid_purify<C>, grid, C::THREADS, args,
+                                            C::SMEM, st));
+  int r[2] = {-1, 0};
+  CUDA_TRY(ctx, cudaMemcpyAsync(r, w.result, 8, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (r[0] == -2) return fail(ctx, SGB_E_CUDA, "a bounded wait of the purification loop gave up");
+  *products = r[0];
+  *xbuf = r[1];
+  return SGB_OK;
+}
+
 // P (packed) from the full F in T by purification (the recursion and limits of purify.cuh);
 // *products = number of products, or -1 when it did not converge (the caller diagonalises).
-// mixed: X and the products in FP32 (SSYRK) while tr(X - X^2) >= kPurifyMixedSwitch, then X is
-// widened to FP64 and the recursion finishes with FP64 products, so the result carries FP64
-// idempotency; the FP32 phase only perturbs the occupied subspace at the 1e-7 level, which
-// enters the energy at second order.
+// The FP64 recursion runs on the device in one launch (grid_purify.cuh).  mixed: X and the
+// products in FP32 (SSYRK) while tr(X - X^2) >= kPurifyMixedSwitch, then X is widened to FP64
+// and the device loop finishes with FP64 products, so the result carries FP64 idempotency; the
+// FP32 phase only perturbs the occupied subspace at the 1e-7 level, which enters the energy at
+// second order.
 int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   const MolView v = mol_view(mol->b);
   GridWork& w = mol->gw;
   cudaStream_t st = ctx->stream;
   const int n = v.nao;
   const int64_t nn = (int64_t)n * n;
-  if (!ctx->blas) {
-    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS)
-      return fail(ctx, SGB_E_CUDA, "cublasCreate failed");
-  }
-  if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS)
-    return fail(ctx, SGB_E_CUDA, "cublasSetStream failed");
-  double* X = w.G;
   double* sc = w.scalars;  // [2] lo, [3] hi, [4] tr X, [5] ||X||^2
   const int nbr = grid_blocks(ctx, 32LL * n);
   k_pur_bounds<<<nbr, kGridThreads, 0, st>>>(n, v.T, w.partial);
@@ -950,64 +1035,62 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
     int rc = grid_lanczos_bounds(ctx, mol, sc + 2);
     if (rc) return rc;
   }
-  const int nb = grid_blocks(ctx, nn);
-  float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
-  float* Y32 = X32 + nn;
-  bool fp32 = mixed;
-  bool fused = !fp32;  // the FP64 kernels finish their sums themselves
-  if (fp32)
+  const int bm = gp_tile(n, ctx->num_sms);
+  const int np = (n + bm - 1) / bm * bm;
+  const int nbp = grid_blocks(ctx, (int64_t)np * np);
+  *products = -1;
+  int it0 = 0, rc;
+  if (mixed) {
+    if (!ctx->blas) {
+      if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS)
+        return fail(ctx, SGB_E_CUDA, "cublasCreate failed");
+    }
+    if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS)
+      return fail(ctx, SGB_E_CUDA, "cublasSetStream failed");
+    const int nb = grid_blocks(ctx, nn);
+    float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
+    float* Y32 = X32 + nn;
     k_pur_init32<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X32, w.partial);
-  else
-    k_pur_init<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X, w.partial, w.count, sc + 4);
-  double t[2];
-  auto sums = [&]() -> int {
-    if (!fused) {
+    double t[2];
+    auto sums = [&]() -> int {
       k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
       k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nb, nb, sc + 5);
-    }
-    CUDA_TRY(ctx, cudaGetLastError());
-    CUDA_TRY(ctx, cudaMemcpyAsync(t, sc + 4, 16, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    return SGB_OK;
-  };
-  int rc = sums();
-  if (rc) return rc;
-  const double one = 1.0, zero = 0.0, n_o = (double)v.nocc;
-  const float onef = 1.0f, zerof = 0.0f;
-  int tail = -1;
-  *products = -1;
-  for (int it = 0; it <= kPurifyMaxIter; ++it) {
-    if (!(fabs(t[0]) < INFINITY) || !(fabs(t[1]) < INFINITY)) return SGB_OK;
-    if (fp32 && t[0] - t[1] < kPurifyMixedSwitch) {
-      k_pur_widen<<<nb, kGridThreads, 0, st>>>(nn, X32, X, n, w.partial);
-      if ((rc = sums())) return rc;
-      fp32 = false;
-      fused = true;
-    }
-    if (tail < 0 && t[0] - t[1] < kPurifyIdem) tail = kPurifyTail;
-    if (tail == 0) {
-      if (fabs(t[0] - n_o) < kPurifyTraceTol) {
-        k_pur_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, X, v.P, ctx->damping);
-        CUDA_TRY(ctx, cudaGetLastError());
-        *products = it;
-      }
+      CUDA_TRY(ctx, cudaGetLastError());
+      CUDA_TRY(ctx, cudaMemcpyAsync(t, sc + 4, 16, cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(ctx, cudaStreamSynchronize(st));
       return SGB_OK;
-    }
-    if (tail > 0) --tail;
-    if (it == kPurifyMaxIter) break;
-    const int sq = fabs(t[1] - n_o) < fabs(2.0 * t[0] - t[1] - n_o);
-    if (fp32) {
+    };
+    if ((rc = sums())) return rc;
+    const double n_o = (double)v.nocc;
+    const float onef = 1.0f, zerof = 0.0f;
+    for (;; ++it0) {
+      if (!(fabs(t[0]) < INFINITY) || !(fabs(t[1]) < INFINITY)) return SGB_OK;
+      if (t[0] - t[1] < kPurifyMixedSwitch) break;
+      if (it0 == kPurifyMaxIter) return SGB_OK;
+      const int sq = fabs(t[1] - n_o) < fabs(2.0 * t[0] - t[1] - n_o);
       if (cublasSsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &onef, X32, n, &zerof,
                       Y32, n) != CUBLAS_STATUS_SUCCESS)
         return fail(ctx, SGB_E_CUDA, "cublasSsyrk failed (n = %d)", n);
       k_pur_update32<<<nb, kGridThreads, 0, st>>>(n, X32, Y32, sq, w.partial);
-    } else {
-      if (cublasDsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &one, X, n, &zero,
-                      w.X2, n) != CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, SGB_E_CUDA, "cublasDsyrk failed (n = %d)", n);
-      k_pur_update<<<nb, kGridThreads, 0, st>>>(n, X, w.X2, sq, w.partial, w.count, sc + 4);
+      if ((rc = sums())) return rc;
     }
-    if ((rc = sums())) return rc;
+    k_gp_widen32<<<nbp, kGridThreads, 0, st>>>(n, np, X32, w.G, w.partial, w.count, sc + 4);
+  } else {
+    k_gp_init<<<nbp, kGridThreads, 0, st>>>(n, np, v.T, sc + 2, w.G, w.partial, w.count, sc + 4);
+  }
+  CUDA_TRY(ctx, cudaGetLastError());
+  int prod = -1, xbuf = 0;
+  if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, &prod, &xbuf);
+  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, &prod, &xbuf);
+  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, &prod, &xbuf);
+  if (rc) return rc;
+  if (prod >= 0) {
+    const double* X = xbuf ? w.X2 : w.G;
+    k_gp_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, np, X, v.P, ctx->damping);
+    CUDA_TRY(ctx, cudaGetLastError());
+    w.xbuf = xbuf;
+    w.xnp = np;
+    *products = prod;
   }
   return SGB_OK;
 }
@@ -1065,12 +1148,16 @@ int diis_step(sgb_ctx* ctx, sgb_mol* mol, DiisState& ds) {
   double* Eh = w.diis + depth * nn;  // depth error matrices
   const int slot = ds.next;
   CUDA_TRY(ctx, cudaMemcpyAsync(Fh + slot * nn, v.T, 8 * nn, cudaMemcpyDeviceToDevice, st));
-  const double two = 2.0, zero = 0.0;  // C = F (2X) = F P
-  if (cublasDgemm(ctx->blas, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &two, v.T, n, w.G, n, &zero,
-                  w.X2, n) != CUBLAS_STATUS_SUCCESS)
-    return fail(ctx, SGB_E_CUDA, "cublasDgemm failed (DIIS error)");
+  // C = F X (X = P / 2, symmetric) and e = C - C^T: the commutator up to the factor 2, to which
+  // the DIIS coefficients are insensitive.  The purified X (padded) is unpadded into the free
+  // buffer, C overwrites X (P was already written from it).
   const int nb = grid_blocks(ctx, nn);
-  k_commutator<<<nb, kGridThreads, 0, st>>>(n, w.X2, Eh + slot * nn);
+  double* Xp = w.xbuf ? w.X2 : w.G;
+  double* Xu = w.xbuf ? w.G : w.X2;
+  k_gp_unpad<<<nb, kGridThreads, 0, st>>>(n, w.xnp, Xp, Xu);
+  const dim3 gemm_grid((n + kGemmTile - 1) / kGemmTile, (n + kGemmTile - 1) / kGemmTile);
+  k_grid_gemm<<<gemm_grid, 256, 0, st>>>(n, v.T, Xu, Xp);
+  k_commutator<<<nb, kGridThreads, 0, st>>>(n, Xp, Eh + slot * nn);
   ds.count = std::min(ds.count + 1, depth);
   ds.next = (slot + 1) % depth;
   for (int j = 0; j < ds.count; ++j) {
@@ -1333,6 +1420,7 @@ int sgb_ctx_create(int device, size_t budget, sgb_ctx** out) {
   if ((e = cudaSetDevice(device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = upload_tables()) != cudaSuccess || (e = prepare_kernels()) != cudaSuccess ||
+      (e = prepare_grid_purify()) != cudaSuccess ||
       (e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess) {
     delete c;
     return SGB_E_CUDA;

@@ -25,7 +25,7 @@ struct GridBarrier {
 
 constexpr long long kBarrierSpins = 1LL << 26;  // x >= 64 ns sleep: several seconds
 
-__device__ bool grid_barrier(const GridBarrier& b) {
+__device__ bool grid_barrier(GridBarrier b) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = b.gen;

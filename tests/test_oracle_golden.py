@@ -67,3 +67,16 @@ def test_readme_pyridine(oracle_mod):
     assert f"{r['E_el']:.6g}" == "-3360.88"
     assert f"{r['E_cc']:.6g}" == "2444.36"
     assert f"{r['E_el'] + r['E_cc']:.6g}" == "-916.525"
+
+
+def test_restatement_matches_reference_on_c100h202(oracle_mod):
+    """The C restatement against the reference build's own C100H202 run (302 atoms, 602 AOs,
+    tol 1e-6 eV; tests/golden/make_golden.py --c2, about 80 minutes of serial reference time):
+    the same 10 steps, per-step energies, final F and P."""
+    g = np.load(os.path.join(GOLDEN, "reference_c100h202.npz"))
+    o = oracle_mod.scf(g["Z"], g["xyz"], tol=1e-6)
+    assert o["n_iter"] == int(g["n_iter"]) == 10
+    np.testing.assert_allclose(o["energies"], g["energies"], rtol=0, atol=1e-8)
+    np.testing.assert_allclose(o["F"], g["F"], rtol=0, atol=1e-10)
+    np.testing.assert_allclose(o["P"], g["P"], rtol=0, atol=1e-11)
+    assert abs(o["E_cc"] - float(g["E_cc"])) < 1e-8
