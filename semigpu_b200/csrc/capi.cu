@@ -933,7 +933,12 @@ int grid_lanczos_bounds(sgb_ctx* ctx, sgb_mol* mol, double* lohi) {
 
 // Tile configuration of the device purification loop for order n: the largest tile that
 // still gives every SM work (two tiles per SM for the 128 x 128 tile, one for 64 x 64).
+// SGB_GRID_TILE=32, 64 or 128 overrides the choice (for tile-size sweeps).
 int gp_tile(int n, int num_sms) {
+  if (const char* env = getenv("SGB_GRID_TILE")) {
+    const int t = atoi(env);
+    if (t == GpLarge::BM || t == GpMid::BM || t == GpSmall::BM) return t;
+  }
   auto tiles = [](int n, int bm) { const int64_t t = (n + bm - 1) / bm; return t * (t + 1) / 2; };
   if (tiles(n, GpLarge::BM) >= 2LL * num_sms) return GpLarge::BM;
   if (tiles(n, GpMid::BM) >= num_sms) return GpMid::BM;
@@ -962,7 +967,8 @@ cudaError_t gp_prepare() {
 
 cudaError_t prepare_grid_purify() {
   cudaError_t e;
-  if ((e = gp_prepare<GpLarge>()) || (e = gp_prepare<GpMid>()) || (e = gp_prepare<GpSmall>()))
+  if ((e = gp_prepare<GpLarge>()) || (e = gp_prepare<GpMid>()) || (e = gp_prepare<GpSmall>()) ||
+      (e = gp_prepare<GpLargeAlt1>()) || (e = gp_prepare<GpLargeAlt2>()))
     return e;
   return cudaSuccess;
 }
@@ -1080,7 +1086,11 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   }
   CUDA_TRY(ctx, cudaGetLastError());
   int prod = -1, xbuf = 0;
-  if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, &prod, &xbuf);
+  const char* var = getenv("SGB_GRID_VARIANT");  // alternatives of the 128 tile (sweeps)
+  const int vsel = var ? atoi(var) : 0;
+  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, &prod, &xbuf);
+  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, &prod, &xbuf);
+  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, &prod, &xbuf);
   else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, &prod, &xbuf);
   else rc = gp_launch<GpSmall>(ctx, mol, np, it0, &prod, &xbuf);
   if (rc) return rc;
