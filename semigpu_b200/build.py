@@ -58,7 +58,7 @@ def host_up_to_date() -> bool:
 
 def build(verbose: bool = False, force: bool = False) -> str:
     if force or not up_to_date():
-        cmd = [NVCC, *FLAGS, SRC, "-o", OUT, "-lcublas"]
+        cmd = [NVCC, *FLAGS, SRC, "-o", OUT]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
             print(" ".join(cmd), flush=True)

@@ -1,6 +1,5 @@
 // C ABI of the engine (include/semigpu_b200.h).  One translation unit: the device tables live
 // in this TU's constant bank, and every kernel is instantiated here.
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,6 +15,7 @@
 #include "../../include/semigpu_b200.h"
 #include "batch_scf.cuh"
 #include "grid_purify.cuh"
+#include "grid_purify32.cuh"
 #include "grid_scf.cuh"
 #include "layout.h"
 #include "mndo_tables.cuh"
@@ -90,7 +90,6 @@ struct sgb_ctx {
   int max_sweeps = 0;          // Jacobi sweeps per eigensolve (0: the path's default)
   long long wait_spins = -1;   // polls of a bounded device wait (< 0: the default bound)
   double damping = 0.0;        // density damping factor (0: off)
-  cublasHandle_t blas = nullptr;  // created on first use (the products of grid purification)
   // Timing events for batches, created with the context and recycled: cudaEventCreate waits
   // for the kernels running on the device, which would stall a batch built while another
   // context's long launch runs.
@@ -965,8 +964,26 @@ cudaError_t gp_prepare() {
   return cudaSuccess;
 }
 
+cudaError_t prepare_grid_purify32() {
+  static bool done[kMaxDevices] = {};
+  static std::mutex m;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(m);
+  if (!done[dev]) {
+    e = cudaFuncSetAttribute(k_grid_purify32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kTfSmem);
+    if (e != cudaSuccess) return e;
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
 cudaError_t prepare_grid_purify() {
   cudaError_t e;
+  if ((e = prepare_grid_purify32())) return e;
   if ((e = gp_prepare<GpLarge>()) || (e = gp_prepare<GpMid>()) || (e = gp_prepare<GpSmall>()) ||
       (e = gp_prepare<GpLargeAlt1>()) || (e = gp_prepare<GpLargeAlt2>()))
     return e;
@@ -976,12 +993,13 @@ cudaError_t prepare_grid_purify() {
 // One cooperative launch of the device purification loop on X_0 in buffer 0 (padded order
 // np, sums at t0); *products and *xbuf from its result.
 template <class C>
-int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, int* products, int* xbuf) {
+int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, bool swap, int* products,
+              double** xout) {
   GridWork& w = mol->gw;
   cudaStream_t st = ctx->stream;
   const int nocc = mol->b->desc[0].nocc;
   CUtensorMap maps[2];
-  double* bufs[2] = {w.G, w.X2};
+  double* bufs[2] = {swap ? w.X2 : w.G, swap ? w.G : w.X2};  // X_0 in bufs[0]
   for (int k = 0; k < 2; ++k)
     if (!make_tensor_map_2d(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, bufs[k], np, np, np,
                             C::BM, kGpK))
@@ -1016,7 +1034,58 @@ int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, int* products, int* x
   CUDA_TRY(ctx, cudaStreamSynchronize(st));
   if (r[0] == -2) return fail(ctx, SGB_E_CUDA, "a bounded wait of the purification loop gave up");
   *products = r[0];
-  *xbuf = r[1];
+  *xout = bufs[r[1] & 1];
+  return SGB_OK;
+}
+
+// The FP32 phase of the mixed form on the tensor cores (grid_purify32.cuh), from X_0 split into
+// set 0 (G); *products = products done when tr(X - X^2) fell below the switch point (or -1),
+// *set = the set (0: G, 1: X2) holding X.
+int gp32_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int* products, int* set) {
+  GridWork& w = mol->gw;
+  cudaStream_t st = ctx->stream;
+  float* H[2] = {reinterpret_cast<float*>(w.G), reinterpret_cast<float*>(w.X2)};
+  const int64_t nn = (int64_t)np * np;
+  float* L[2] = {H[0] + nn, H[1] + nn};
+  CUtensorMap maps[4];
+  for (int k = 0; k < 2; ++k)
+    if (!make_tensor_map_2d(&maps[2 * k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, H[k], np, np, np,
+                            kTfBM, kTfK) ||
+        !make_tensor_map_2d(&maps[2 * k + 1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L[k], np, np, np,
+                            kTfBM, kTfK))
+      return fail(ctx, SGB_E_CUDA, "tensor maps of the FP32 purification buffers (np = %d)", np);
+  CUDA_TRY(ctx, prepare_grid_purify32());
+  int per_sm = 0;
+  CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_purify32,
+                                                              kTfThreads, kTfSmem));
+  if (per_sm < 1) return fail(ctx, SGB_E_CUDA, "FP32 purification kernel does not fit an SM");
+  const int nt = np / kTfBM;
+  const int grid = (int)std::min<int64_t>((int64_t)nt * (nt + 1) / 2,
+                                          std::min<int64_t>((int64_t)per_sm * ctx->num_sms,
+                                                            kPartialMax / 4));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.bar, 0, 8, st));
+  CUDA_TRY(ctx, cudaMemsetAsync(w.err, 0, 4, st));
+  GridPurify32Args a;
+  a.np = np;
+  a.nocc = mol->b->desc[0].nocc;
+  a.hi[0] = H[0]; a.hi[1] = H[1];
+  a.lo[0] = L[0]; a.lo[1] = L[1];
+  a.partial = w.partial;
+  a.t0 = w.scalars + 4;
+  a.result = w.result;
+  a.bar = GridBarrier{w.bar, w.bar + 1, w.err, barrier_spins(ctx), 0u};
+  a.spins = ctx->wait_spins >= 0 ? ctx->wait_spins : kMbarSpins;
+  a.switch_at = kPurifyMixedSwitch;
+  void* args[] = {&maps[0], &maps[1], &maps[2], &maps[3], &a};
+  CUDA_TRY(ctx, cudaLaunchCooperativeKernel((void*)k_grid_purify32, grid, kTfThreads, args,
+                                            kTfSmem, st));
+  int r[2] = {-1, 0};
+  CUDA_TRY(ctx, cudaMemcpyAsync(r, w.result, 8, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  if (r[0] == -2)
+    return fail(ctx, SGB_E_CUDA, "a bounded wait of the FP32 purification loop gave up");
+  *products = r[0];
+  *set = r[1] & 1;
   return SGB_OK;
 }
 
@@ -1032,7 +1101,6 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   GridWork& w = mol->gw;
   cudaStream_t st = ctx->stream;
   const int n = v.nao;
-  const int64_t nn = (int64_t)n * n;
   double* sc = w.scalars;  // [2] lo, [3] hi, [4] tr X, [5] ||X||^2
   const int nbr = grid_blocks(ctx, 32LL * n);
   k_pur_bounds<<<nbr, kGridThreads, 0, st>>>(n, v.T, w.partial);
@@ -1046,59 +1114,41 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   const int nbp = grid_blocks(ctx, (int64_t)np * np);
   *products = -1;
   int it0 = 0, rc;
+  bool swap = false;  // X_0 of the FP64 loop in X2 instead of G
   if (mixed) {
-    if (!ctx->blas) {
-      if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, SGB_E_CUDA, "cublasCreate failed");
-    }
-    if (cublasSetStream(ctx->blas, st) != CUBLAS_STATUS_SUCCESS)
-      return fail(ctx, SGB_E_CUDA, "cublasSetStream failed");
-    const int nb = grid_blocks(ctx, nn);
-    float* X32 = reinterpret_cast<float*>(w.X2);  // FP32 phase: X and X^2 share X2's space
-    float* Y32 = X32 + nn;
-    k_pur_init32<<<nb, kGridThreads, 0, st>>>(n, v.T, sc + 2, X32, w.partial);
-    double t[2];
-    auto sums = [&]() -> int {
-      k_reduce_sum<<<1, 256, 0, st>>>(w.partial, nb, sc + 4);
-      k_reduce_sum<<<1, 256, 0, st>>>(w.partial + nb, nb, sc + 5);
-      CUDA_TRY(ctx, cudaGetLastError());
-      CUDA_TRY(ctx, cudaMemcpyAsync(t, sc + 4, 16, cudaMemcpyDeviceToHost, st));
-      CUDA_TRY(ctx, cudaStreamSynchronize(st));
-      return SGB_OK;
-    };
-    if ((rc = sums())) return rc;
-    const double n_o = (double)v.nocc;
-    const float onef = 1.0f, zerof = 0.0f;
-    for (;; ++it0) {
-      if (!(fabs(t[0]) < INFINITY) || !(fabs(t[1]) < INFINITY)) return SGB_OK;
-      if (t[0] - t[1] < kPurifyMixedSwitch) break;
-      if (it0 == kPurifyMaxIter) return SGB_OK;
-      const int sq = fabs(t[1] - n_o) < fabs(2.0 * t[0] - t[1] - n_o);
-      if (cublasSsyrk(ctx->blas, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, n, n, &onef, X32, n, &zerof,
-                      Y32, n) != CUBLAS_STATUS_SUCCESS)
-        return fail(ctx, SGB_E_CUDA, "cublasSsyrk failed (n = %d)", n);
-      k_pur_update32<<<nb, kGridThreads, 0, st>>>(n, X32, Y32, sq, w.partial);
-      if ((rc = sums())) return rc;
-    }
-    k_gp_widen32<<<nbp, kGridThreads, 0, st>>>(n, np, X32, w.G, w.partial, w.count, sc + 4);
+    // FP32 phase on the tensor cores (TF32 x 3) from X_0 split into hi / lo in G, then X widened
+    // into whichever of G / X2 does not hold it, where the FP64 loop continues
+    const int np32 = (int)grid_pad(n);
+    float* H0 = reinterpret_cast<float*>(w.G);
+    k_gp_init32<<<grid_blocks(ctx, (int64_t)np32 * np32), kGridThreads, 0, st>>>(
+        n, np32, v.T, sc + 2, H0, H0 + (int64_t)np32 * np32, w.partial, w.count, sc + 4);
+    CUDA_TRY(ctx, cudaGetLastError());
+    int set = 0;
+    if ((rc = gp32_launch(ctx, mol, np32, &it0, &set))) return rc;
+    if (it0 < 0) return SGB_OK;  // not finite / no convergence: the caller diagonalises
+    const float* Hs = reinterpret_cast<const float*>(set ? w.X2 : w.G);
+    const float* Ls = Hs + (int64_t)np32 * np32;
+    swap = set == 0;
+    k_gp_widen_split<<<nbp, kGridThreads, 0, st>>>(n, np32, Hs, Ls, np, swap ? w.X2 : w.G,
+                                                    w.partial, w.count, sc + 4);
   } else {
     k_gp_init<<<nbp, kGridThreads, 0, st>>>(n, np, v.T, sc + 2, w.G, w.partial, w.count, sc + 4);
   }
   CUDA_TRY(ctx, cudaGetLastError());
-  int prod = -1, xbuf = 0;
+  int prod = -1;
+  double* Xf = nullptr;
   const char* var = getenv("SGB_GRID_VARIANT");  // alternatives of the 128 tile (sweeps)
   const int vsel = var ? atoi(var) : 0;
-  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, &prod, &xbuf);
-  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, &prod, &xbuf);
-  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, &prod, &xbuf);
-  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, &prod, &xbuf);
-  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, &prod, &xbuf);
+  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, swap, &prod, &Xf);
+  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, swap, &prod, &Xf);
+  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, swap, &prod, &Xf);
+  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, swap, &prod, &Xf);
+  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, swap, &prod, &Xf);
   if (rc) return rc;
   if (prod >= 0) {
-    const double* X = xbuf ? w.X2 : w.G;
-    k_gp_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, np, X, v.P, ctx->damping);
+    k_gp_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, np, Xf, v.P, ctx->damping);
     CUDA_TRY(ctx, cudaGetLastError());
-    w.xbuf = xbuf;
+    w.xbuf = Xf == w.X2 ? 1 : 0;
     w.xnp = np;
     *products = prod;
   }
@@ -1608,7 +1658,6 @@ int sgb_ctx_destroy(sgb_ctx* ctx) {
     std::lock_guard<std::mutex> lock(ctx->spare_mutex);
     release_spares(ctx, 0, 0);
   }
-  if (ctx->blas) cublasDestroy(ctx->blas);
   for (int k = 0; k < kNumClasses; ++k) {
     if (ctx->aux[k]) cudaStreamDestroy(ctx->aux[k]);
     if (ctx->joined[k]) cudaEventDestroy(ctx->joined[k]);

@@ -177,10 +177,10 @@ __global__ void k_energy_partials(int64_t np, const double* __restrict__ H,
 }
 
 // ------------------------------------------------------------------------------------------
-// Purification on the whole GPU: the recursion of purify.cuh for one large molecule.  The
-// products X^2 are symmetric rank-n updates issued by the host loop (cuBLAS DSYRK, lower
-// triangle, column-major); these kernels build X_0, apply the chosen branch and reduce tr X and
-// ||X||_F^2 -- block partials, then one fixed-order pass, so the sums are deterministic.
+// Purification on the whole GPU: the recursion of purify.cuh for one large molecule runs in
+// the device loops of grid_purify.cuh (FP64) and grid_purify32.cuh (the mixed form's FP32
+// phase); the pieces here are the spectral bounds of F and the fixed-order finishing of block
+// sums (deterministic).
 
 // Block partials of (a, b); the last block to finish adds them up in a fixed order into
 // out[0..1] (so the totals do not depend on which block is last) and resets *count, which must
@@ -255,93 +255,10 @@ __global__ void k_pur_bounds_reduce(const double* partial, int nb, double* lohi)
   }
 }
 
-// X_0 = (hi I - F) / (hi - lo); block partials of tr X (partial[blk]) and ||X||^2
-// (partial[gridDim + blk]).
-__global__ void k_pur_init(int n, const double* __restrict__ F, const double* lohi, double* X,
-                           double* partial, unsigned* count, double* out) {
-  const double lo = lohi[0], hi = lohi[1], inv = 1.0 / (hi - lo);
-  const int64_t nn = (int64_t)n * n;
-  double s1 = 0.0, s2 = 0.0;
-  for (int64_t t = gtid(); t < nn; t += gstride()) {
-    const int64_t i = t / n, j = t - i * n;
-    const double v = ((i == j ? hi : 0.0) - F[t]) * inv;
-    X[t] = v;
-    if (i == j) s1 += v;
-    s2 = fma(v, v, s2);
-  }
-  finalize_sums2(s1, s2, partial, count, out);
-}
 
-// X <- X2 (sq) or 2X - X2 on the lower triangle of X2 (column-major), mirrored; partial sums
-// of the new tr X and ||X||^2 as in k_pur_init.
-__global__ void k_pur_update(int n, double* X, const double* __restrict__ X2, int sq,
-                             double* partial, unsigned* count, double* out) {
-  const int64_t nn = (int64_t)n * n;
-  double s1 = 0.0, s2 = 0.0;
-  for (int64_t t = gtid(); t < nn; t += gstride()) {
-    const int64_t j = t / n, i = t - j * n;  // element (i, j) at i + j n
-    if (i < j) continue;
-    const double x2 = X2[t];
-    const double v = sq ? x2 : fma(2.0, X[t], -x2);
-    X[t] = v;
-    if (i != j) X[j + i * n] = v;
-    if (i == j) s1 += v;
-    s2 = fma(i == j ? v : 2.0 * v, v, s2);
-  }
-  finalize_sums2(s1, s2, partial, count, out);
-}
 
-// Mixed precision: the same two kernels on an FP32 X (products on the tensor cores as
-// split-BF16 FP32 emulation); the sums stay FP64.
-__global__ void k_pur_init32(int n, const double* __restrict__ F, const double* lohi, float* X,
-                             double* partial) {
-  const double lo = lohi[0], hi = lohi[1], inv = 1.0 / (hi - lo);
-  const int64_t nn = (int64_t)n * n;
-  double s1 = 0.0, s2 = 0.0;
-  for (int64_t t = gtid(); t < nn; t += gstride()) {
-    const int64_t i = t / n, j = t - i * n;
-    const float v = (float)(((i == j ? hi : 0.0) - F[t]) * inv);
-    X[t] = v;
-    if (i == j) s1 += v;
-    s2 = fma((double)v, (double)v, s2);
-  }
-  write_block_partial(s1, partial);
-  __syncthreads();
-  write_block_partial(s2, partial + gridDim.x);
-}
 
-__global__ void k_pur_update32(int n, float* X, const float* __restrict__ X2, int sq,
-                               double* partial) {
-  const int64_t nn = (int64_t)n * n;
-  double s1 = 0.0, s2 = 0.0;
-  for (int64_t t = gtid(); t < nn; t += gstride()) {
-    const int64_t j = t / n, i = t - j * n;
-    if (i < j) continue;
-    const float x2 = X2[t];
-    const float v = sq ? x2 : fmaf(2.0f, X[t], -x2);
-    X[t] = v;
-    if (i != j) X[j + i * n] = v;
-    if (i == j) s1 += v;
-    s2 = fma(i == j ? (double)v : 2.0 * v, (double)v, s2);
-  }
-  write_block_partial(s1, partial);
-  __syncthreads();
-  write_block_partial(s2, partial + gridDim.x);
-}
 
-// FP32 X -> FP64 X for the refinement products, with its sums.
-__global__ void k_pur_widen(int64_t nn, const float* X32, double* X, int n, double* partial) {
-  double s1 = 0.0, s2 = 0.0;
-  for (int64_t t = gtid(); t < nn; t += gstride()) {
-    const double v = (double)X32[t];
-    X[t] = v;
-    if (t / n == t % n) s1 += v;
-    s2 = fma(v, v, s2);
-  }
-  write_block_partial(s1, partial);
-  __syncthreads();
-  write_block_partial(s2, partial + gridDim.x);
-}
 
 // Lanczos steps of the spectral bounds (purify.cuh), for one large molecule: the host keeps
 // the coefficients and the loop; vectors q, q_prev, w of length n on the device.
@@ -424,16 +341,6 @@ __global__ void k_lincomb(int64_t nn, LinComb lc, double* out) {
   }
 }
 
-// P (packed lower triangle) = 2 X
-// P = 2 X (packed), mixed with the previous P by the damping factor d when d > 0.
-__global__ void k_pur_density(int n, const double* X, double* P, double d) {
-  for (int64_t t = gtid(); t < tri(n); t += gstride()) {
-    int i, j;
-    tri_inverse(t, i, j);
-    const double p = 2.0 * X[(int64_t)i * n + j];
-    P[t] = d > 0.0 ? fma(d, P[t] - p, p) : p;
-  }
-}
 
 // ------------------------------------------------------------------------------------------
 // Dense pieces of the eigensolve (column-major n x n, ld n)
