@@ -21,13 +21,16 @@
 //    the first step it is warm-started from the previous eigenvectors, which the new F barely
 //    mixes, so it needs few sweeps.
 #pragma once
+#include "dmma_tiles.cuh"
 #include "fock_block.cuh"
+#include "tf32_tiles.cuh"
 #include "purify.cuh"
 #include "scf_block.cuh"
 
 namespace sgb {
 
 constexpr int kBatchJacobiSweeps = 40;
+constexpr int kWorkMaps = 6;  // tensor maps per molecule above nao 160
 
 struct BatchArgs {
   int nmol;
@@ -47,6 +50,9 @@ struct BatchArgs {
   double* T;
   double* eig;
   double* W;        // work matrices (X and its partner, or G) of the molecules above nao 160
+  // tensor maps of the work matrices of the molecules above nao 160, kWorkMaps per molecule:
+  // X and its partner as FP64, then the TF32 hi / lo parts of the two sets of the mixed form
+  const CUtensorMap* wmaps = nullptr;
   double* e_el;
   double* e_cc;
   int* n_iter;
@@ -437,8 +443,31 @@ __device__ void run_molecule(const BatchArgs& a, int mi, double* smem) {
         const double* Xr = smem;
         if constexpr (PLACE == 2) {  // X and its partner in the global work matrix
           double* Xo = nullptr;
-          prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq, red,
-                                         &Xo);
+          if constexpr (NT == BpCfg::THREADS) {
+            if (a.wmaps && d.wmap >= 0) {
+              // TMA-staged tiles; the ring follows the kernel's other shared memory
+              unsigned char* ring = reinterpret_cast<unsigned char*>(
+                  smem + a.mat_doubles + extra_doubles(a.nmax));
+              const CUtensorMap* maps = a.wmaps + kWorkMaps * d.wmap;
+              bool tensor = false;
+              if constexpr ((MX & FEAT_TENSOR) != 0) {
+                // mixed form: TF32 tensor-core phase, FP64 finish
+                tensor = a.solver == SOLVER_PURIFY_MIXED;
+                if (tensor)
+                  prod = block_purify_tiles32<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n),
+                                                  maps, ring, wq, red, &Xo, a.wait_spins);
+              }
+              if (!tensor)
+                prod = block_purify_tiles<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n),
+                                              maps, maps + 1, ring, wq, red, &Xo, a.wait_spins);
+            } else {
+              prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq,
+                                             red, &Xo);
+            }
+          } else {
+            prod = block_purify_global<NT>(Ffull, n, m.nocc, m.W, m.W + purify_doubles(n), wq, red,
+                                           &Xo);
+          }
           Xr = Xo;
         } else {
           bool tensor = false;

@@ -147,6 +147,7 @@ struct sgb_batch {
   int* d_hb = nullptr;
   double *d_ints = nullptr, *d_H = nullptr, *d_P = nullptr, *d_F = nullptr;
   double *d_V = nullptr, *d_T = nullptr, *d_eig = nullptr, *d_W = nullptr;
+  CUtensorMap* d_maps = nullptr;  // work-matrix tensor maps of the molecules above nao 160
   double *d_eel = nullptr, *d_ecc = nullptr;
   int *d_niter = nullptr, *d_conv = nullptr, *d_status = nullptr;
   unsigned long long *d_tb = nullptr, *d_te = nullptr;
@@ -429,6 +430,7 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->desc.resize(nmol);
   b->natoms.assign(natoms, natoms + nmol);
   int64_t atom0 = 0, blk0 = 0, pk0 = 0, sq0 = 0, ao0 = 0, w0 = 0;
+  int nmaps = 0;
   std::vector<int8_t> slot;
   std::vector<int> first, hb;
   std::vector<int64_t> row_off;
@@ -470,9 +472,12 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
     d.sq0 = sq0;
     d.ao0 = ao0;
     d.w0 = w0;
+    d.wmap = -1;
+    d.pad_ = 0;
     if (nao > kGsmemMax) {  // Jacobi's G (n x n) or purification's X and Y
       const int64_t need = std::max<int64_t>((int64_t)nao * nao, 2 * (int64_t)purify_doubles(nao));
       w0 += (need + 31) / 32 * 32;
+      d.wmap = nmaps++;
     }
     blk0 += (roff + 31) / 32 * 32;
     pk0 += (tri(nao) + 31) / 32 * 32;
@@ -513,7 +518,8 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
                o_ecc = take(8 * nmol), o_nit = take(4 * nmol), o_conv = take(4 * nmol),
                o_stat = take(4 * nmol), o_tb = take(8 * nmol), o_te = take(8 * nmol),
                o_stage = take(8 * (size_t)kStageSlots * nmol),
-               o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0);
+               o_hist = take(hist_stride > 0 ? 8 * (size_t)hist_stride * nmol : 0),
+               o_maps = take(sizeof(CUtensorMap) * kWorkMaps * (size_t)nmaps);
   b->bytes = off;
   cudaError_t e = cudaSuccess;
   if (ctx->pool && !ctx->pool_busy && off <= ctx->pool_bytes) {
@@ -554,6 +560,34 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
   b->d_te = (unsigned long long*)(base + o_te);
   b->d_stage = (unsigned long long*)(base + o_stage);
   b->d_hist = hist_stride > 0 ? (double*)(base + o_hist) : nullptr;
+  b->d_maps = nmaps ? (CUtensorMap*)(base + o_maps) : nullptr;
+  // tensor maps of the work matrices X and Y of the molecules above nao 160 (n16 x n16, row
+  // stride n16 + 8): FP64 X and Y in 64-row boxes of 16 doubles, then for the mixed form the
+  // TF32 hi / lo parts of the two sets (set 0 in X's slot, set 1 in Y's; n16 x n16 floats, row
+  // stride n16 + 8 floats, 128-row boxes of 32 floats); a molecule whose maps cannot be encoded
+  // keeps the purification without TMA
+  std::vector<CUtensorMap> maps(kWorkMaps * (size_t)nmaps);
+  for (int m = 0; m < nmol && nmaps; ++m) {
+    MolDesc& d = b->desc[m];
+    if (d.wmap < 0) continue;
+    const int n16 = purify_n16(d.nao), ld = purify_ld(d.nao);
+    double* X = b->d_W + d.w0;
+    double* Y = X + purify_doubles(d.nao);
+    CUtensorMap* mp = &maps[kWorkMaps * (size_t)d.wmap];
+    bool ok = make_tensor_map_2d(&mp[0], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, X, n16, n16, ld,
+                                 BpCfg::BM, kGpK) &&
+              make_tensor_map_2d(&mp[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, Y, n16, n16, ld,
+                                 BpCfg::BM, kGpK);
+    for (int set = 0; set < 2 && ok; ++set) {
+      float* H = reinterpret_cast<float*>(set ? Y : X);
+      float* L = H + (int64_t)n16 * ld;
+      ok = make_tensor_map_2d(&mp[2 + 2 * set], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, H, n16, n16, ld,
+                              kTfBM, kTfK) &&
+           make_tensor_map_2d(&mp[3 + 2 * set], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, L, n16, n16, ld,
+                              kTfBM, kTfK);
+    }
+    if (!ok) d.wmap = -1;
+  }
   cudaStream_t st = ctx->stream;
   const HostCopy ups[] = {{b->d_desc, b->desc.data(), sizeof(MolDesc) * nmol},
                           {b->d_order, b->order.data(), sizeof(int) * (size_t)nmol},
@@ -561,8 +595,9 @@ int build_batch(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const d
                           {b->d_xyz, xyz, 24 * (size_t)NA},
                           {b->d_first, first.data(), 4 * (size_t)NA},
                           {b->d_row_off, row_off.data(), 8 * (size_t)NA},
-                          {b->d_hb, hb.data(), 4 * (size_t)NA}};
-  if ((e = upload(ctx, ups, 7, st)) != cudaSuccess ||
+                          {b->d_hb, hb.data(), 4 * (size_t)NA},
+                          {b->d_maps, maps.data(), sizeof(CUtensorMap) * maps.size()}};
+  if ((e = upload(ctx, ups, 8, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(b->d_status, 0, 4 * nmol, st)) != cudaSuccess ||
       (e = take_event(ctx, &b->ev0)) != cudaSuccess || (e = take_event(ctx, &b->ev1)) != cudaSuccess) {
     free_batch(b);
@@ -618,7 +653,7 @@ template <int FEAT>
 cudaError_t prepare_feat(int* c) {
   constexpr int D = FEAT & FEAT_DIIS;
   cudaError_t e;
-  if ((e = kernel_smem_cap<512, 0, D>(c)) || (e = kernel_smem_cap<128, 2, D>(c)) ||
+  if ((e = kernel_smem_cap<512, 0, FEAT>(c)) || (e = kernel_smem_cap<128, 2, D>(c)) ||
       (e = kernel_smem_cap<256, 2, D>(c)) || (e = kernel_smem_cap<256, 3, D>(c)) ||
       (e = kernel_smem_cap<256, 4, D>(c)) || (e = kernel_smem_cap<256, 5, D>(c)) ||
       (e = kernel_smem_cap<512, 2, D>(c)) || (e = kernel_smem_cap<512, 3, FEAT>(c)) ||
@@ -653,12 +688,13 @@ cudaError_t launch_kernel(int num_sms, const BatchArgs& a, size_t smem, cudaStre
   return cudaGetLastError();
 }
 
-// FEAT_TENSOR only reaches the 512-thread classes of nao 65-160 (CR 3-5); FEAT_DIIS all.
+// FEAT_TENSOR only reaches the 512-thread classes of nao 65-160 (CR 3-5) and the class above
+// the shared-memory limit (CR 0); FEAT_DIIS all.
 template <int FEAT>
 cudaError_t launch_feat(int num_sms, const BatchArgs& a, int cr, int threads, size_t smem,
                         cudaStream_t st) {
   constexpr int D = FEAT & FEAT_DIIS;
-  if (cr == 0) return launch_kernel<512, 0, D>(num_sms, a, smem, st);
+  if (cr == 0) return launch_kernel<512, 0, FEAT>(num_sms, a, smem, st);
   if (threads == 128 && cr == 2) return launch_kernel<128, 2, D>(num_sms, a, smem, st);
   if (threads == 512) {
     switch (cr) {
@@ -703,7 +739,7 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
   a.hb = b->d_hb;
   a.ints = b->d_ints;
   a.H = b->d_H; a.P = b->d_P; a.F = b->d_F;
-  a.V = b->d_V; a.T = b->d_T; a.eig = b->d_eig; a.W = b->d_W;
+  a.V = b->d_V; a.T = b->d_T; a.eig = b->d_eig; a.W = b->d_W; a.wmaps = b->d_maps;
   a.e_el = b->d_eel; a.e_cc = b->d_ecc;
   a.n_iter = b->d_niter; a.converged = b->d_conv; a.status = b->d_status;
   a.hist = b->d_hist; a.hist_stride = b->hist_stride;
@@ -754,7 +790,9 @@ int launch_stages(sgb_ctx* ctx, sgb_batch* b, int stages, double tol, int max_it
       for (int q = 0; q < cnt; ++q)
         ac.mat_doubles = std::max(ac.mat_doubles,
                                   mat_doubles_for(b->desc[b->order[b->class_first[c] + q]].nao));
-    const size_t smem = (ac.mat_doubles + extra_doubles(ac.nmax)) * sizeof(double);
+    size_t smem = (ac.mat_doubles + extra_doubles(ac.nmax)) * sizeof(double);
+    // the class above the shared-memory limit purifies through a TMA ring after the rest
+    if (kClasses[c].cr == 0 && (stages & STAGE_SCF)) smem += kBpRingBytes;
     cudaStream_t cs = ctx->aux[c];
     CUDA_TRY(ctx, cudaStreamWaitEvent(cs, b->ev0, 0));
     const int sms = ctx->sm_limit > 0 ? std::min(ctx->sm_limit, ctx->num_sms) : ctx->num_sms;
@@ -2061,6 +2099,7 @@ int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int
   h.desc.nocc = nel / 2;
   h.desc.nheavy = nheavy;
   h.desc.nblk = roff;  // all offsets of the views below are relative to their own buffers
+  h.desc.wmap = -1;
   h.order = 0;         // counter[] stays zero: it must start at zero every run
   if (cudaMemcpyAsync(base + o_head, &h, sizeof h, cudaMemcpyHostToDevice, st) != cudaSuccess)
     return SGB_E_CUDA;
@@ -2086,6 +2125,7 @@ int sgb_scf_noalloc(int natoms, const int* Z, const double* xyz, double tol, int
   a.T = reinterpret_cast<double*>(base + o_T);
   a.eig = reinterpret_cast<double*>(base + o_eig);
   a.W = nullptr;
+  a.wmaps = nullptr;
   a.e_el = &dr->e_el;
   a.e_cc = &dr->e_cc;
   a.n_iter = &dr->n_iter;

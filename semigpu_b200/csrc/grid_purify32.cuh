@@ -19,16 +19,12 @@
 // its loads and MMAs in flight, gives its tensor memory back and the launch reports -2.
 #pragma once
 #include "grid_purify.cuh"
+#include "tf32_tiles.cuh"
 
 namespace sgb {
 
-constexpr int kTfBM = 128;                  // tile rows = MMA M = MMA N
-constexpr int kTfK = 32;                    // floats per k-block (one 128-byte swizzle row)
 constexpr int kTfStages = 3;
-constexpr int kTfBox = kTfBM * 128;         // one panel part (hi or lo) of one k-block: 16 KB
-constexpr int kTfStageBytes = 4 * kTfBox;   // A hi, A lo, B hi, B lo
 constexpr int kTfThreads = 192;             // warp 0 loads, warp 1 MMAs, warps 2-5 epilogue
-constexpr int kTfTmemCols = 256;            // two 128-column FP32 accumulators
 constexpr size_t kTfSmem = 1024 + (size_t)kTfStages * kTfStageBytes + 256;
 
 struct GridPurify32Args {
@@ -44,35 +40,6 @@ struct GridPurify32Args {
   long long spins;
   double switch_at;    // the phase ends when tr(X - X^2) < switch_at
 };
-
-// Shared-memory matrix descriptor of a K-major operand in the 128-byte swizzle layout TMA
-// writes: 8-row groups 1024 bytes apart (stride byte offset), descriptor version 1, swizzle
-// mode 2 (128 B).  The k-slices of a 128-byte row are addressed by advancing the start address
-// (the swizzle is applied to the absolute shared-memory address, as TMA applied it).
-__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
-__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
-                                          uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_addr(bar))
-               : "memory");
-}
-
-// Splits v into its TF32 head and the FP32 remainder.
-__device__ __forceinline__ void tf32_split(float v, float& h, float& l) {
-  h = __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
-  l = v - h;
-}
 
 __global__ void __launch_bounds__(kTfThreads, 1)
     k_grid_purify32(const __grid_constant__ CUtensorMap mh0, const __grid_constant__ CUtensorMap ml0,

@@ -26,6 +26,8 @@ struct MolDesc {
   int64_t ao0;    // first entry of its per-AO vectors
   int64_t nblk;   // integral doubles owned
   int64_t w0;     // first double of its work matrices in global memory (nao > 160)
+  int wmap;       // its pair of work-matrix tensor maps (nao > 160), or -1
+  int pad_;
 };
 
 // Block offset (relative to the molecule's blk0) of atom pair (A, B), A >= B.

@@ -1,0 +1,345 @@
+// TF32 tensor-core products (tcgen05.mma kind::tf32, accumulators in tensor memory) for the
+// FP32 phase of the mixed-precision purification: X kept split in two TF32 parts, hi = X with
+// the low 13 mantissa bits cleared and lo = X - hi, and X^2 ~ hi hi^T + hi lo^T + lo hi^T (about
+// 21 mantissa bits per product, the accuracy of an FP32 product).  Operands are 128-row panels
+// of hi and lo, K-major, staged by TMA in the 128-byte swizzle.  Used by the whole-GPU loop
+// (grid_purify32.cuh) and by one CTA per molecule (block_purify_tiles32 below, molecules above
+// the shared-memory limit in a batch).
+#pragma once
+#include "dmma_tiles.cuh"
+
+namespace sgb {
+
+constexpr int kTfBM = 128;                  // tile rows = MMA M = MMA N
+constexpr int kTfK = 32;                    // floats per k-block (one 128-byte swizzle row)
+constexpr int kTfBox = kTfBM * 128;         // one panel part (hi or lo) of one k-block: 16 KB
+constexpr int kTfStageBytes = 4 * kTfBox;   // A hi, A lo, B hi, B lo
+constexpr int kTfTmemCols = 256;            // two 128-column FP32 accumulators
+
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte swizzle layout TMA
+// writes: 8-row groups 1024 bytes apart (stride byte offset), descriptor version 1, swizzle
+// mode 2 (128 B).  The k-slices of a 128-byte row are addressed by advancing the start address
+// (the swizzle is applied to the absolute shared-memory address, as TMA applied it).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_addr(bar))
+               : "memory");
+}
+
+// Splits v into its TF32 head and the FP32 remainder.
+__device__ __forceinline__ void tf32_split(float v, float& h, float& l) {
+  h = __uint_as_float(__float_as_uint(v) & 0xFFFFE000u);
+  l = v - h;
+}
+
+
+// ---- one CTA, one molecule ---------------------------------------------------------------
+
+constexpr int kBpTfStages = 2;  // 2 x 64 KB
+constexpr size_t kBpRingBytes =
+    1024 + (kBpRingFp64 > (size_t)kBpTfStages * kTfStageBytes ? kBpRingFp64
+                                                               : (size_t)kBpTfStages * kTfStageBytes) +
+    256;
+// For these orders the FP32 phase's idempotency floor is near 1e-4 (n eigenvalues with FP32-level
+// errors), so it hands over to FP64 at 1e-3, as the whole-GPU form does.
+constexpr double kBpTf32Switch = 1e-3;
+
+// The mixed form of block_purify_tiles for one CTA of 512 threads: X_0 from F in FP64 (slot X),
+// split into TF32 hi / lo in slot Y (set 1; hi then lo, row stride n16 + 8 floats each, so a
+// set fills one slot), then products on the tensor cores while tr(X - X^2) >= kBpTf32Switch --
+// warp 0 loads, warp 1 issues the MMAs into one of two 128-column accumulators, warps 4-7
+// (one thread per tile row) read the accumulator and write the new hi / lo into the other set
+// -- then X widened to FP64 into the slot the last set does not hold and bp_fp64_loop finishes.
+// maps: [0] X slot FP64, [1] Y slot FP64, [2] / [3] hi / lo of set 0 (slot X), [4] / [5] hi / lo
+// of set 1 (slot Y); 128-row boxes of 32 floats for the FP32 ones.
+template <int NT>
+__device__ __noinline__ int block_purify_tiles32(const double* F, int n, int nocc, double* X,
+                                                 double* Y, const CUtensorMap* maps,
+                                                 unsigned char* ring_raw, double* lz, double* red,
+                                                 double** Xout, long long spins) {
+  static_assert(NT == 512, "warps 4-7 read the four tensor-memory lane quarters");
+  constexpr int NW = NT / 32;
+  const int ld = purify_ld(n), n16 = purify_n16(n);
+  const int64_t part = (int64_t)n16 * ld;  // floats of one TF32 part (hi or lo)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ volatile int s_abort;
+  __shared__ uint32_t s_tmem;
+  double t1, t2;
+  purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
+  float* hs[2] = {reinterpret_cast<float*>(X), reinterpret_cast<float*>(Y)};
+  {  // X_0 (FP64) -> set 1 (hi, lo) with its sums
+    double s1 = 0.0, s2 = 0.0;
+    float* H = hs[1];
+    float* L = H + part;
+    for (int64_t t = threadIdx.x; t < (int64_t)n16 * n16; t += NT) {
+      const int r = (int)(t / n16), c = (int)(t - (int64_t)r * n16);
+      float h, l;
+      tf32_split((float)X[(int64_t)r * ld + c], h, l);
+      H[(int64_t)r * ld + c] = h;
+      L[(int64_t)r * ld + c] = l;
+      const double x = (double)h + (double)l;
+      if (r == c) s1 += x;
+      s2 = fma(x, x, s2);
+    }
+    block_sum2<NT>(s1, s2, red);
+    t1 = s1;
+    t2 = s2;
+  }
+  unsigned char* tiles = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(ring_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kBpTfStages * kTfStageBytes);
+  uint64_t* empty = full + kBpTfStages;
+  uint64_t* accf = empty + kBpTfStages;
+  uint64_t* acce = accf + 2;
+  uint64_t* drain = acce + 2;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kBpTfStages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf + b, 1);
+      mbar_init(acce + b, 4);
+    }
+    mbar_init(drain, 1);
+    mbar_fence_init();
+    s_abort = 0;
+  }
+  if (warp == 1)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_addr(&s_tmem)),
+                 "r"(kTfTmemCols));
+  fence_proxy_async_global();  // set 1 is read by TMA
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = s_tmem;
+  const int nt = (n16 + kTfBM - 1) / kTfBM, T = nt * (nt + 1) / 2;
+  const int kblocks = (n16 + kTfK - 1) / kTfK;
+  const uint32_t idesc = umma_idesc_tf32(kTfBM, kTfBM);
+  long long issued = 0, consumed = 0, mma_tiles = 0, epi_tiles = 0;
+  int cur = 1, it = 0;
+  bool ok = true;
+  for (;; ++it) {
+    if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY) || it == kPurifyMaxIter) {
+      ok = false;
+      break;
+    }
+    if (t1 - t2 < kBpTf32Switch) break;
+    const double n_o = (double)nocc;
+    const bool sq = fabs(t2 - n_o) < fabs(2.0 * t1 - t2 - n_o);
+    const CUtensorMap* mh = maps + 2 + 2 * cur;
+    const CUtensorMap* ml = mh + 1;
+    const float* Xh = hs[cur];
+    const float* Xl = Xh + part;
+    float* Yh = hs[cur ^ 1];
+    float* Yl = Yh + part;
+    double s1 = 0.0, s2 = 0.0;
+    if (warp == 0) {
+      if (lane == 0) {  // ---- loader ----
+        for (int t = 0; t < T && !s_abort; ++t) {
+          int I, J;
+          tri_inverse(t, I, J);
+          for (int kb = 0; kb < kblocks; ++kb) {
+            const int s = (int)(issued % kBpTfStages);
+            if (issued >= kBpTfStages &&
+                !mbar_wait(empty + s, (uint32_t)((issued / kBpTfStages - 1) & 1), spins)) {
+              s_abort = 1;
+              break;
+            }
+            unsigned char* st = tiles + s * kTfStageBytes;
+            mbar_arrive_expect_tx(full + s, kTfStageBytes);
+            tma_load_2d(st, mh, kb * kTfK, I * kTfBM, full + s);
+            tma_load_2d(st + kTfBox, ml, kb * kTfK, I * kTfBM, full + s);
+            tma_load_2d(st + 2 * kTfBox, mh, kb * kTfK, J * kTfBM, full + s);
+            tma_load_2d(st + 3 * kTfBox, ml, kb * kTfK, J * kTfBM, full + s);
+            ++issued;
+          }
+        }
+      }
+    } else if (warp == 1) {
+      if (lane == 0) {  // ---- MMA issue ----
+        for (int t = 0; t < T && !s_abort; ++t) {
+          const int b = (int)(mma_tiles & 1);
+          const long long use = mma_tiles >> 1;
+          if (use >= 1 && !mbar_wait(acce + b, (uint32_t)((use - 1) & 1), spins)) {
+            s_abort = 1;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t d = tmem + (uint32_t)(b * kTfBM);
+          for (int kb = 0; kb < kblocks; ++kb) {
+            const int s = (int)(consumed % kBpTfStages);
+            if (!mbar_wait(full + s, (uint32_t)((consumed / kBpTfStages) & 1), spins)) {
+              s_abort = 1;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t base = smem_addr(tiles + s * kTfStageBytes);
+#pragma unroll
+            for (int ks = 0; ks < kTfK / 8; ++ks) {
+              const uint32_t off = (uint32_t)ks * 32;
+              const uint64_t ah = umma_desc_sw128(base + off);
+              const uint64_t al = umma_desc_sw128(base + kTfBox + off);
+              const uint64_t bh = umma_desc_sw128(base + 2 * kTfBox + off);
+              const uint64_t bl = umma_desc_sw128(base + 3 * kTfBox + off);
+              umma_tf32(d, ah, bh, idesc, (kb | ks) ? 1u : 0u);
+              umma_tf32(d, ah, bl, idesc, 1u);
+              umma_tf32(d, al, bh, idesc, 1u);
+            }
+            umma_commit(empty + s);
+            ++consumed;
+          }
+          if (s_abort) break;
+          umma_commit(accf + b);
+          ++mma_tiles;
+        }
+      }
+    } else if (warp >= 4 && warp < 8) {
+      // ---- epilogue: one thread per tile row (tensor-memory lane 32 (warp & 3) + lane) ----
+      const int quad = warp & 3;
+      const int lr = 32 * quad + lane;
+      for (int t = 0; t < T && !s_abort; ++t) {
+        int I, J;
+        tri_inverse(t, I, J);
+        const int b = (int)(epi_tiles & 1);
+        if (!mbar_wait(accf + b, (uint32_t)((epi_tiles >> 1) & 1), spins)) {
+          s_abort = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int r = I * kTfBM + lr;
+        const int64_t row = (int64_t)r * ld;
+        const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(b * kTfBM);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kTfBM; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(taddr + (uint32_t)c0, v);  // every lane: the load is warp-collective
+          const int cb = J * kTfBM + c0;
+          if (r >= n16 || cb >= n16 || r < cb) continue;  // past the matrix / above the diagonal
+#pragma unroll
+          for (int g4 = 0; g4 < 4; ++g4) {
+            const int c = cb + 4 * g4;  // n16 is a multiple of 16: c .. c + 3 all inside
+            const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
+            const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
+            const float old[4] = {oh.x + ol.x, oh.y + ol.y, oh.z + ol.z, oh.w + ol.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const int ce = c + e;
+              if (r < ce) continue;
+              const float d2 = __uint_as_float(v[4 * g4 + e]);
+              float h, l;
+              tf32_split(sq ? d2 : fmaf(2.0f, old[e], -d2), h, l);
+              __stcg(Yh + row + ce, h);
+              __stcg(Yl + row + ce, l);
+              const double x = (double)h + (double)l;
+              if (r == ce) {
+                s1 += x;
+                s2 = fma(x, x, s2);
+              } else {
+                __stcg(Yh + (int64_t)ce * ld + r, h);
+                __stcg(Yl + (int64_t)ce * ld + r, l);
+                s2 = fma(2.0 * x, x, s2);
+              }
+            }
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(acce + b);
+        ++epi_tiles;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+      s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    }
+    double* pr = red + 32 * (it & 1);
+    if (lane == 0) { pr[warp] = s1; pr[16 + warp] = s2; }
+    fence_proxy_async_global();  // the new set is read by TMA in the next product
+    __syncthreads();
+    if (s_abort) {
+      ok = false;
+      break;
+    }
+    s1 = 0.0;
+    s2 = 0.0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) { s1 += pr[k]; s2 += pr[16 + k]; }
+    t1 = s1;
+    t2 = s2;
+    cur ^= 1;
+  }
+  if (s_abort) {
+    // loads and MMAs still in flight write this CTA's shared and tensor memory: wait for them
+    // (bounded) before the memory is given back
+    if (warp == 0 && lane == 0)
+      for (long long c = issued - kBpTfStages; c < issued; ++c)
+        if (c >= 0)
+          mbar_wait(full + (int)(c % kBpTfStages), (uint32_t)((c / kBpTfStages) & 1), kMbarSpins);
+    if (warp == 1 && lane == 0) {
+      umma_commit(drain);
+      mbar_wait(drain, 0, kMbarSpins);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTfTmemCols));
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kBpTfStages; ++s) {
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(full + s)));
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(empty + s)));
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(accf + b)));
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(acce + b)));
+    }
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(drain)));
+  }
+  __syncthreads();
+  if (!ok) {
+    *Xout = X;
+    return -1;
+  }
+  // ---- widen the last set into the other slot (FP64) and finish in FP64 ----
+  double* Xd = cur ? X : Y;  // the slot that does not hold set `cur`
+  double* Yd = cur ? Y : X;
+  const CUtensorMap* mXd = cur ? maps : maps + 1;
+  const CUtensorMap* mYd = cur ? maps + 1 : maps;
+  {
+    const float* H = hs[cur];
+    const float* L = H + part;
+    double s1 = 0.0, s2 = 0.0;
+    for (int64_t t = threadIdx.x; t < (int64_t)n16 * n16; t += NT) {
+      const int r = (int)(t / n16), c = (int)(t - (int64_t)r * n16);
+      const int64_t a = (int64_t)r * ld + c, bb = (int64_t)c * ld + r;
+      const double v = 0.5 * (((double)H[a] + (double)L[a]) + ((double)H[bb] + (double)L[bb]));
+      Xd[a] = v;
+      if (r == c) s1 += v;
+      s2 = fma(v, v, s2);
+    }
+    block_sum2<NT>(s1, s2, red);
+    t1 = s1;
+    t2 = s2;
+  }
+  return bp_fp64_loop<NT>(Xd, Yd, mXd, mYd, n, nocc, ring_raw, red, Xout, spins, it, t1, t2);
+}
+
+}  // namespace sgb

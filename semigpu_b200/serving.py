@@ -45,9 +45,9 @@ def device_bytes(mol: Geometry) -> int:
     nblk = 100 * heavy * (heavy + 1) // 2 + 10 * heavy * light + light * (light + 1) // 2
     n = mol.nao
     squares = 2 * n * n
-    if n > SMEM_MAX_NAO:  # work matrices X and Y of purification, n16 x (n16 + 4) each
+    if n > SMEM_MAX_NAO:  # work matrices X and Y of purification, n16 x (n16 + 8) each
         n16 = (n + 15) // 16 * 16
-        squares += max(n * n, 2 * n16 * (n16 + 4))
+        squares += max(n * n, 2 * n16 * (n16 + 8))
     return 8 * (nblk + 3 * n * (n + 1) // 2 + squares + n) + 64 * mol.natoms + 256
 
 

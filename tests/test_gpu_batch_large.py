@@ -80,3 +80,29 @@ def test_c100h202_in_batch_against_oracle(gpu_ctx, oracle_mod):
     assert r["n_iter"][0] == o["n_iter"]
     assert abs(r["E_el"][0] - o["E_el"]) < 1e-6
     assert abs(r["E_cc"][0] - o["E_cc"]) < 1e-6
+
+
+def test_large_mixed_tensor_core_against_oracle(oracle_mod):
+    """Mixed form above nao 160 in the batch (one CTA per molecule): the TF32 tensor-core phase
+    on TMA-staged hi / lo panels, then the FP64 tile loop; every molecule within 1e-4 eV of the
+    FP64 oracle, with no Jacobi fallback."""
+    rng = np.random.default_rng(19)
+    mols = [geo.alkane(27, rng), geo.polyene(40, rng), geo.alkane(50, rng), geo.polyene(90, rng)]
+    assert [m.nao for m in mols] == [164, 202, 302, 452]
+    ctx = sg.Context(0)
+    try:
+        ctx.set_density_solver(sg.SOLVER_PURIFY_MIXED)
+        b = sg.Batch(ctx, mols)
+        b.set_profiling(True)
+        b.run(1e-6)
+        r = b.results()
+        sc = b.stage_cycles()
+        b.close()
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
+    for i, m in enumerate(mols):
+        o = oracle_mod.scf(m.Z, m.xyz, tol=1e-6)
+        assert abs(r["E_tot"][i] - o["E_tot"]) <= 1e-4, (m.nao, r["E_tot"][i] - o["E_tot"])
+        assert abs(r["n_iter"][i] - o["n_iter"]) <= 1
