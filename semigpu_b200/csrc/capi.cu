@@ -1031,7 +1031,7 @@ cudaError_t prepare_grid_purify() {
 // One cooperative launch of the device purification loop on X_0 in buffer 0 (padded order
 // np, sums at t0); *products and *xbuf from its result.
 template <class C>
-int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, bool swap, int* products,
+int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, bool swap, bool mixed, int* products,
               double** xout) {
   GridWork& w = mol->gw;
   cudaStream_t st = ctx->stream;
@@ -1064,6 +1064,7 @@ int gp_launch(sgb_ctx* ctx, sgb_mol* mol, int np, int it0, bool swap, int* produ
   a.bar = GridBarrier{w.bar, w.bar + 1, w.err, barrier_spins(ctx), 0u};
   a.spins = ctx->wait_spins >= 0 ? ctx->wait_spins : kMbarSpins;
   a.it0 = it0;
+  a.mixed_finish = mixed ? 1 : 0;
   void* args[] = {&maps[0], &maps[1], &a};
   CUDA_TRY(ctx, cudaLaunchCooperativeKernel((void*)k_grid_purify<C>, grid, C::THREADS, args,
                                             C::SMEM, st));
@@ -1177,11 +1178,11 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   double* Xf = nullptr;
   const char* var = getenv("SGB_GRID_VARIANT");  // alternatives of the 128 tile (sweeps)
   const int vsel = var ? atoi(var) : 0;
-  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, swap, &prod, &Xf);
-  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, swap, &prod, &Xf);
-  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, swap, &prod, &Xf);
-  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, swap, &prod, &Xf);
-  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, swap, &prod, &Xf);
+  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
+  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
+  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
+  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
+  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
   if (rc) return rc;
   if (prod >= 0) {
     k_gp_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, np, Xf, v.P, ctx->damping);

@@ -223,8 +223,9 @@ __device__ __forceinline__ void gp_product(GpRing& ring, const CUtensorMap* map,
 // ---- one CTA, one molecule: the recursion with X and its partner in global memory ----------
 
 // 64 x 64 tiles, 16 warps of 16 x 16 (the batch kernel's 512 threads at its 128-register cap),
-// 2 k-blocks per stage, 3 stages (96 KB).
-using BpCfg = GpCfg<64, 4, 4, 2, 3>;
+// 3 k-blocks per stage, 2 stages (96 KB).  148 alkanes of 164-902 AOs, one CTA each, FP64:
+// 861 ms against 921 ms with 2 k-blocks x 3 stages and 897 ms with 4 x 2.
+using BpCfg = GpCfg<64, 4, 4, 3, 2>;
 constexpr size_t kBpRingFp64 = (size_t)BpCfg::STAGES * BpCfg::STAGE_BYTES;
 
 // The FP64 recursion on X (n16 x n16, row stride n16 + 8, global memory) from product it0 with
@@ -236,7 +237,8 @@ template <int NT>
 __device__ __noinline__ int bp_fp64_loop(double* X, double* Y, const CUtensorMap* mX,
                                          const CUtensorMap* mY, int n, int nocc,
                                          unsigned char* ring_raw, double* red, double** Xout,
-                                         long long spins, int it0, double t1, double t2) {
+                                         long long spins, int it0, double t1, double t2,
+                                         bool mixed_finish) {
   static_assert(NT == BpCfg::THREADS, "one warp per 16 x 16 warp tile of the 64 x 64 tile");
   constexpr int NW = NT / 32;
   const int ld = purify_ld(n), n16 = purify_n16(n);
@@ -264,8 +266,12 @@ __device__ __noinline__ int bp_fp64_loop(double* X, double* Y, const CUtensorMap
   int tail = -1, result = -1;
   for (int it = it0;; ++it) {
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) break;
-    if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
-    if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    if (mixed_finish) {  // the mixed form: done at kMixedIdemFinal, no tail
+      if (fabs(t1 - t2) < kMixedIdemFinal) tail = 0;
+    } else {
+      if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+      if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    }
     if (tail == 0) {
       if (fabs(t1 - (double)nocc) < kPurifyTraceTol) result = it;
       break;
@@ -322,7 +328,8 @@ __device__ __noinline__ int block_purify_tiles(const double* F, int n, int nocc,
                                                long long spins) {
   double t1, t2;
   purify_init<NT>(F, n, X, purify_ld(n), lz, red, t1, t2);
-  return bp_fp64_loop<NT>(X, Y, mapX, mapY, n, nocc, ring_raw, red, Xout, spins, 0, t1, t2);
+  return bp_fp64_loop<NT>(X, Y, mapX, mapY, n, nocc, ring_raw, red, Xout, spins, 0, t1, t2,
+                          false);
 }
 
 }  // namespace sgb

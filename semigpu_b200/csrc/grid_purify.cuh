@@ -39,6 +39,7 @@ struct GridPurifyArgs {
   GridBarrier bar;
   long long spins;   // polls of each mbarrier wait
   int it0;           // products already done (the mixed form's FP32 phase)
+  int mixed_finish;  // the mixed form: done at kMixedIdemFinal, no tail
 };
 
 template <class C>
@@ -78,8 +79,12 @@ __global__ void __launch_bounds__(C::THREADS, 1)
   for (int it = a.it0;; ++it) {
     // ---- the decision of purify_fp64_loop, identical in every thread of every CTA ----
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) { result = -1; break; }
-    if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
-    if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    if (a.mixed_finish) {
+      if (fabs(t1 - t2) < kMixedIdemFinal) tail = 0;
+    } else {
+      if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+      if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    }
     if (tail == 0) {
       result = fabs(t1 - (double)a.nocc) < kPurifyTraceTol ? it : -1;
       break;

@@ -458,6 +458,11 @@ constexpr long long kMbarSpins = 1 << 22;
 // FP32 products until tr(X - X^2) falls below this (3xTF32 keeps X to ~1e-7, so the
 // idempotency error is still well above its FP32 floor of ~1e-5 here)
 constexpr double kPurifyTensorSwitch = 1e-4;
+// The mixed form's FP64 finish (above the shared-memory limit and on the whole GPU) ends once
+// tr(X - X^2) < kMixedIdemFinal, with no tail: every eigenvalue of X is then within 1e-10 of 0
+// or 1, which moves E_el by at most 1e-10 x sum |eigenvalues of F| (below 1e-5 eV up to 1024
+// AOs), well inside the form's 1e-4 eV, and saves the FP64 products of the tail.
+constexpr double kMixedIdemFinal = 1e-10;
 
 // Splits v into its TF32 head and the FP32 remainder at canonical position idx.
 __device__ __forceinline__ void put_split(float* hi, float* lo, int idx, float v) {

@@ -339,7 +339,8 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
     t1 = s1;
     t2 = s2;
   }
-  return bp_fp64_loop<NT>(Xd, Yd, mXd, mYd, n, nocc, ring_raw, red, Xout, spins, it, t1, t2);
+  return bp_fp64_loop<NT>(Xd, Yd, mXd, mYd, n, nocc, ring_raw, red, Xout, spins, it, t1, t2,
+                          true);
 }
 
 }  // namespace sgb

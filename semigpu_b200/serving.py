@@ -65,7 +65,7 @@ class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
                  batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
-                 big_sm_share: float = 0.6, solver: int | None = None):
+                 big_sm_share: float = 0.85, solver: int | None = None):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
         queue of molecules above nao 160 (at least one slot stays with the small queue); their
@@ -244,6 +244,8 @@ def main(argv=None):
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--big-slots", type=int, default=2)
     ap.add_argument("--hbm-gb", type=float, default=40.0)
+    ap.add_argument("--big-share", type=float, default=0.85,
+                    help="fraction of the SMs the large-molecule workers' launches may use")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mixed", action="store_true",
                     help="mixed precision (TF32 tensor-core products, FP64 finish)")
@@ -260,6 +262,7 @@ def main(argv=None):
             times.append(t)
         arrivals = list(zip(times, geo.batch_c3(len(times), seed=args.seed)))
     srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)),
+                 big_sm_share=args.big_share,
                  solver=SOLVER_PURIFY_MIXED if args.mixed else SOLVER_PURIFY)
     try:
         srv.replay([(0.001 * i, m) for i, (_, m) in enumerate(arrivals[:40])])  # warm-up
@@ -267,7 +270,7 @@ def main(argv=None):
     finally:
         srv.close()
     out = {"workload": args.workload, "rate_per_s": args.rate, "duration_s": args.duration,
-           "precision": "mixed" if args.mixed else "fp64",
+           "precision": "mixed" if args.mixed else "fp64", "big_share": args.big_share,
            "all": stats(done),
            "small": stats([r for r in done if r.mol.nao <= SMEM_MAX_NAO]),
            "large": stats([r for r in done if r.mol.nao > SMEM_MAX_NAO]),
