@@ -160,13 +160,17 @@ def load_traffic():
 # ------------------------------------------------------------------------------------------
 # CPU reference timing
 
-def stratified(mols, k, offset=0):
-    """k molecules at evenly spaced quantiles of nao, largest first (so a process pool
-    schedules them longest-job-first)."""
+def stratified_index(mols, k, offset=0):
+    """Indices of k molecules at evenly spaced quantiles of nao, largest first (so a process
+    pool schedules them longest-job-first)."""
     idx = np.argsort([m.nao for m in mols], kind="stable")
     pos = np.linspace(0, len(mols) - 1, k).round().astype(int)
     pos = np.clip(pos + offset, 0, len(mols) - 1)
-    return [mols[int(idx[p])] for p in pos[::-1]]
+    return [int(idx[p]) for p in pos[::-1]]
+
+
+def stratified(mols, k, offset=0):
+    return [mols[i] for i in stratified_index(mols, k, offset)]
 
 
 def _ref_one(args):
@@ -425,8 +429,8 @@ def run_ours(args):
                  "max_abs_dE_total_eV": float(dE.max()), "tolerance_eV": 1e-4,
                  "n_iter_changed": int(np.sum(rm["n_iter"] != res["n_iter"])),
                  "all_converged": bool(np.all(rm["converged"])),
-                 "form": "TF32 tcgen05 products (3xTF32) for nao 65-160, FP64 elsewhere and "
-                         "for the finish of every purification"}
+                 "form": "TF32 tcgen05 products (3xTF32) above nao 64, FP64 below and for the "
+                         "finish of every purification"}
     if rank == 0:
         peak, peak_src = fp64_peak_tflops(torch)
         flops = algorithmic_flops(mols, res["n_iter"])
@@ -488,14 +492,57 @@ def run_ours(args):
         served_mixed = serving.stats(mix_done)
         served_mixed["max_abs_dE_total_eV"] = float(max(
             abs(a.result["E_tot"] - b.result["E_tot"]) for a, b in zip(mix_done, srv_done)))
-        served_mixed["precision"] = "TF32 tcgen05 products for nao 65-160, FP64 finish"
+        served_mixed["precision"] = "TF32 tcgen05 products for nao above 64, FP64 finish"
+        # config-5 stream: 2000 requests/s of the batch composition with alkanes to C150H302
+        # (nao <= 902), mixed precision, split by small (nao <= 160) and large requests; each
+        # request's error against the FP64 result of the same molecule on a sample
+        c5_dur = 10.0
+        c5 = geo.serving_c5(rate=2000.0, duration_s=c5_dur, seed=0)
+        srv = serving.Server(device=local, slots=4, big_slots=2, hbm_budget=40 << 30, tol=TOL,
+                             solver=sg.SOLVER_PURIFY_MIXED)
+        try:
+            srv.replay([(0.001 * i, m) for i, (_, m) in enumerate(c5[:40])])  # warm-up
+            c5_done = srv.replay(c5)
+        finally:
+            srv.close()
+        small_r = [r for r in c5_done if r.mol.nao <= serving.SMEM_MAX_NAO]
+        large_r = [r for r in c5_done if r.mol.nao > serving.SMEM_MAX_NAO]
+        pick = stratified_index([r.mol for r in c5_done], 256)
+        ref64 = sg.run_molecules(ctx, [c5_done[i].mol for i in pick], tol=TOL)
+        dE5 = np.abs(np.array([c5_done[i].result["E_tot"] for i in pick]) - ref64["E_tot"])
+        serving_c5 = {
+            "rate_per_s": 2000.0, "duration_s": c5_dur, "precision": "mixed",
+            "composition": "config 5: batch composition with alkanes CnH2n+2 n=1..150 "
+                           "(nao <= 902), seeded Poisson arrivals",
+            "all": serving.stats(c5_done), "small_nao_le_160": serving.stats(small_r),
+            "large_nao_gt_160": serving.stats(large_r),
+            "large_arrival_rate_per_s": len(large_r) / c5_dur,
+            "max_abs_dE_total_eV_vs_fp64": float(dE5.max()),
+            "dE_sample": f"{len(pick)} requests stratified by nao, against an FP64 batch run",
+            "slots": 4, "big_slots": 2, "big_sm_share": 0.85}
         # CPU baseline: the reference build on the host cores, bounded sample
         cpu = None
         if reference_kind():
             cores = os.cpu_count() or 1
-            csample = stratified(mols, max(cores, 160))
-            dt, cpu_s, _ = reference_queue(csample, cores)
+            cidx = stratified_index(mols, max(cores, 160))
+            csample = [mols[i] for i in cidx]
+            dt, cpu_s, ref_out = reference_queue(csample, cores)
             cpu = cpu_baseline_record(csample, cores, dt, cpu_s, "the same batch")
+            # the reference's own energies for these molecules: the error of the FP64 and of the
+            # mixed-precision batch results against them
+            e_ref = np.array([o[0] for o in ref_out])
+            it_ref = np.array([o[1] for o in ref_out])
+            d64 = np.abs(res["E_tot"][cidx] - e_ref)
+            cpu["parity_on_sample"] = {
+                "molecules": len(cidx), "max_abs_dE_total_eV_fp64": float(d64.max()),
+                "n_iter_equal_fp64": int(np.sum(res["n_iter"][cidx] == it_ref))}
+            if mixed is not None:
+                dmx = np.abs(rm["E_tot"][cidx] - e_ref)
+                mixed["vs_reference_sample"] = {
+                    "molecules": len(cidx), "max_abs_dE_total_eV": float(dmx.max()),
+                    "median_abs_dE_total_eV": float(np.median(dmx)),
+                    "within_tolerance": bool(dmx.max() <= 1e-4),
+                    "reference": "the reference build's E_tot (cpu_baseline leg)"}
         nat_total = int(natoms.sum())
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -514,6 +561,7 @@ def run_ours(args):
                                          "energy, device clock"},
             "mixed_precision": mixed,
             "serving_mixed": served_mixed,
+            "serving_c5": serving_c5,
             "diis": diis,
             "plain_fp64_gpu": {"value": plain, "unit": UNIT,
                                "p50_ms": 1e3 * statistics.median(plain_lat),
