@@ -70,11 +70,12 @@ const char *sgb_status_string(int status);
  *     same aufbau projector; a Jacobi eigensolve replaces it for a step where it does not
  *     converge, and gives the eigenpairs when they are asked for);
  *   SGB_SOLVER_JACOBI -- warm-started Jacobi eigensolves every step;
- *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: for one large molecule (the grid path,
- *     nao > 160) the purification products run in FP32 until the recursion is near idempotent
- *     and finish in FP64 (Fock, energies and the convergence test stay FP64); in a batch,
- *     molecules of 65-160 AOs run the FP32-level products on the tcgen05 tensor cores (TF32,
- *     split in two parts) before the FP64 finish, other sizes keep FP64 products.
+ *   SGB_SOLVER_PURIFY_MIXED -- the mixed-precision form: the purification products run on the
+ *     tcgen05 tensor cores at FP32-level accuracy (TF32, X split in two parts) until the
+ *     recursion is near idempotent and finish in FP64 (Fock, energies and the convergence test
+ *     stay FP64), for batched molecules above 64 AOs (below, FP64 products throughout) and for
+ *     one molecule on the whole GPU from about 2000 AOs (below, FP64 products with the mixed
+ *     form's earlier exit); results within 1e-4 eV of the FP64 form.
  * The environment variable SGB_DENSITY_SOLVER=jacobi or =mixed changes the default (also for
  * sgb_scf_noalloc). */
 #define SGB_SOLVER_PURIFY 0

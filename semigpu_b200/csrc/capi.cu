@@ -1154,7 +1154,11 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   *products = -1;
   int it0 = 0, rc;
   bool swap = false;  // X_0 of the FP64 loop in X2 instead of G
-  if (mixed) {
+  // the tensor-core phase works in 128 x 128 tiles: below one tile per SM (about 2000 AOs) it
+  // would leave most SMs idle, and the FP64 loop (smaller tiles) is faster; the mixed form then
+  // keeps only its FP64 exit
+  const int64_t nt128 = ((int64_t)n + kTfBM - 1) / kTfBM;
+  if (mixed && nt128 * (nt128 + 1) / 2 >= ctx->num_sms) {
     // FP32 phase on the tensor cores (TF32 x 3) from X_0 split into hi / lo in G, then X widened
     // into whichever of G / X2 does not hold it, where the FP64 loop continues
     const int np32 = (int)grid_pad(n);

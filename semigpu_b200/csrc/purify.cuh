@@ -39,6 +39,11 @@ constexpr double kPurifyTraceTol = 1e-6;
 constexpr int kPurifyMaxN16 = 160;  // largest padded order held in one CTA's shared memory
 // Mixed precision (grid path): FP32 products until tr(X - X^2) falls below this, FP64 after.
 constexpr double kPurifyMixedSwitch = 1e-3;
+// The mixed form's FP64 finish (every size that runs the tensor-core phase) ends once
+// tr(X - X^2) < kMixedIdemFinal, with no tail: every eigenvalue of X is then within 1e-10 of 0
+// or 1, which moves E_el by at most 1e-10 x sum |eigenvalues of F| (below 1e-5 eV up to 1024
+// AOs), well inside the form's 1e-4 eV, and saves the FP64 products of the tail.
+constexpr double kMixedIdemFinal = 1e-10;
 
 // Spectral bounds.  Gershgorin discs are always valid but loose (about 2.5x the width of the
 // spectrum for these Fock matrices), and every doubling of the interval costs TC2 about two
@@ -380,12 +385,16 @@ __device__ __noinline__ void purify_step(double* X, int n16, int ld, bool sq, do
 // The recursion from the current X (trace t1, squared norm t2) on, products numbered from it0.
 template <int NT>
 __device__ int purify_fp64_loop(double* X, int n16, int ld, int nocc, double* red, double t1,
-                                double t2, int it0) {
+                                double t2, int it0, bool mixed_finish = false) {
   int tail = -1;
   for (int it = it0; it <= kPurifyMaxIter; ++it) {
     if (!(fabs(t1) < INFINITY) || !(fabs(t2) < INFINITY)) return -1;
-    if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
-    if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    if (mixed_finish) {  // the mixed form: done at kMixedIdemFinal, no tail
+      if (fabs(t1 - t2) < kMixedIdemFinal) tail = 0;
+    } else {
+      if (tail < 0 && fabs(t1 - t2) < kPurifyIdem) tail = kPurifyTail;
+      if (fabs(t1 - t2) < kPurifyIdemFinal) tail = 0;
+    }
     if (tail == 0) return fabs(t1 - (double)nocc) < kPurifyTraceTol ? it : -1;
     if (tail > 0) --tail;
     if (it == kPurifyMaxIter) break;
@@ -458,11 +467,6 @@ constexpr long long kMbarSpins = 1 << 22;
 // FP32 products until tr(X - X^2) falls below this (3xTF32 keeps X to ~1e-7, so the
 // idempotency error is still well above its FP32 floor of ~1e-5 here)
 constexpr double kPurifyTensorSwitch = 1e-4;
-// The mixed form's FP64 finish (above the shared-memory limit and on the whole GPU) ends once
-// tr(X - X^2) < kMixedIdemFinal, with no tail: every eigenvalue of X is then within 1e-10 of 0
-// or 1, which moves E_el by at most 1e-10 x sum |eigenvalues of F| (below 1e-5 eV up to 1024
-// AOs), well inside the form's 1e-4 eV, and saves the FP64 products of the tail.
-constexpr double kMixedIdemFinal = 1e-10;
 
 // Splits v into its TF32 head and the FP32 remainder at canonical position idx.
 __device__ __forceinline__ void put_split(float* hi, float* lo, int idx, float v) {
@@ -672,7 +676,7 @@ __device__ __noinline__ int block_purify_mixed(const double* F, int n, int nocc,
   }
   for (int t = threadIdx.x; t < n16 * 4; t += NT) X[(t >> 2) * ld + n16 + (t & 3)] = 0.0;  // pad
   block_sum2<NT>(s1, s2, red);
-  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it);
+  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it, true);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -913,7 +917,7 @@ __device__ __noinline__ int block_purify_mixed_wide(const double* F, int n, int 
   }
   for (int t = threadIdx.x; t < n16 * 4; t += NT) X[(t >> 2) * ld + n16 + (t & 3)] = 0.0;  // pad
   block_sum2<NT>(s1, s2, red);
-  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it);
+  return purify_fp64_loop<NT>(X, n16, ld, nocc, red, s1, s2, it, true);
 }
 
 // Above nao 160 X does not fit in shared memory: X and Y (n16 x n16, row stride n16 + 8) live
