@@ -205,9 +205,13 @@ __global__ void __launch_bounds__(kTfThreads, 1)
 #pragma unroll
           for (int g4 = 0; g4 < 4; ++g4) {
             const int c = cb + 4 * g4;
-            const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
-            const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
-            const float old[4] = {oh.x + ol.x, oh.y + ol.y, oh.z + ol.z, oh.w + ol.w};
+            // the old X only enters the 2X - X^2 branch
+            float old[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (!sq) {
+              const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
+              const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
+              old[0] = oh.x + ol.x; old[1] = oh.y + ol.y; old[2] = oh.z + ol.z; old[3] = oh.w + ol.w;
+            }
             float nh[4], nl[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {

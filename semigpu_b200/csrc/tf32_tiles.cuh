@@ -233,9 +233,13 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
 #pragma unroll
           for (int g4 = 0; g4 < 4; ++g4) {
             const int c = cb + 4 * g4;  // n16 is a multiple of 16: c .. c + 3 all inside
-            const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
-            const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
-            const float old[4] = {oh.x + ol.x, oh.y + ol.y, oh.z + ol.z, oh.w + ol.w};
+            // the old X only enters the 2X - X^2 branch
+            float old[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            if (!sq) {
+              const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
+              const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
+              old[0] = oh.x + ol.x; old[1] = oh.y + ol.y; old[2] = oh.z + ol.z; old[3] = oh.w + ol.w;
+            }
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const int ce = c + e;
