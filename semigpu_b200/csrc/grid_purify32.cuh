@@ -10,10 +10,11 @@
 // Per CTA: warp 0 loads (TMA, 128-byte swizzle, K-major: one k-block = 32 floats per row of
 // the A-panel hi / lo and B-panel hi / lo boxes, 64 KB per ring stage); warp 1 issues the MMAs
 // (one thread) into one of two 128-column accumulators and commits each stage back to the
-// loader and each finished tile to the epilogue; warps 2-5 (one thread per tile row, the
-// accumulator's tensor-memory lane) read the accumulator, apply X <- X^2 or 2X - X^2, write the
-// new hi / lo (element and mirror) and add to the trace and squared-norm sums, while the MMAs of
-// the next tile run into the other accumulator.  Products are separated by a grid barrier.
+// loader and each finished tile to the epilogue; warps 2-13 (one thread per tile row, the
+// accumulator's tensor-memory lane, three warps per row splitting its columns) read the
+// accumulator, apply X <- X^2 or 2X - X^2, write the new hi / lo (element and mirror) and add
+// to the trace and squared-norm sums, while the MMAs of the next tile run into the other
+// accumulator.  Products are separated by a grid barrier.
 //
 // Every wait is bounded (the context's wait limit); on a timeout the CTA waits (bounded) for
 // its loads and MMAs in flight, gives its tensor memory back and the launch reports -2.
@@ -24,7 +25,11 @@
 namespace sgb {
 
 constexpr int kTfStages = 3;
-constexpr int kTfThreads = 192;             // warp 0 loads, warp 1 MMAs, warps 2-5 epilogue
+// warp 0 loads, warp 1 issues the MMAs, warps 2-13 run the epilogue: three per quarter of the
+// accumulator's tensor-memory lanes (a warp may read only the quarter warp % 4), each taking a
+// third of the tile's 16-column chunks
+constexpr int kTfThreads = 448;
+constexpr int kTfEpiWarps = 12;
 constexpr size_t kTfSmem = 1024 + (size_t)kTfStages * kTfStageBytes + 256;
 
 struct GridPurify32Args {
@@ -64,7 +69,7 @@ __global__ void __launch_bounds__(kTfThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf + b, 1);
-      mbar_init(acce + b, 4);
+      mbar_init(acce + b, kTfEpiWarps);
     }
     mbar_init(drain, 1);
     mbar_fence_init();
@@ -180,8 +185,10 @@ __global__ void __launch_bounds__(kTfThreads, 1)
         }
       }
     } else {
-      // ---- epilogue: warps 2-5, one thread per tile row (tensor-memory lane) ----
+      // ---- epilogue: warps 2-13, one thread per tile row (tensor-memory lane), a third of the
+      // column chunks per warp ----
       const int quad = warp & 3;  // the tensor-memory lanes this warp may read: 32 quad ..
+      const int part = (warp - 2) >> 2;  // 0, 1, 2
       const int lr = 32 * quad + lane;
       for (int m = 0; m < my_tiles && !s_abort; ++m) {
         int I, J;
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(kTfThreads, 1)
         const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(b * kTfBM);
         const bool diag = I == J;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kTfBM; c0 += 16) {
+        for (int c0 = 16 * part; c0 < kTfBM; c0 += 48) {
           uint32_t v[16];
           tmem_ld16(taddr + (uint32_t)c0, v);
           const int cb = J * kTfBM + c0;

@@ -60,8 +60,9 @@ constexpr double kBpTf32Switch = 1e-3;
 // The mixed form of block_purify_tiles for one CTA of 512 threads: X_0 from F in FP64 (slot X),
 // split into TF32 hi / lo in slot Y (set 1; hi then lo, row stride n16 + 8 floats each, so a
 // set fills one slot), then products on the tensor cores while tr(X - X^2) >= kBpTf32Switch --
-// warp 0 loads, warp 1 issues the MMAs into one of two 128-column accumulators, warps 4-7
-// (one thread per tile row) read the accumulator and write the new hi / lo into the other set
+// warp 0 loads, warp 1 issues the MMAs into one of two 128-column accumulators, warps 4-15
+// (one thread per tile row, three warps per row) read the accumulator and write the new hi / lo
+// into the other set
 // -- then X widened to FP64 into the slot the last set does not hold and bp_fp64_loop finishes.
 // maps: [0] X slot FP64, [1] Y slot FP64, [2] / [3] hi / lo of set 0 (slot X), [4] / [5] hi / lo
 // of set 1 (slot Y); 128-row boxes of 32 floats for the FP32 ones.
@@ -70,7 +71,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
                                                  double* Y, const CUtensorMap* maps,
                                                  unsigned char* ring_raw, double* lz, double* red,
                                                  double** Xout, long long spins) {
-  static_assert(NT == 512, "warps 4-7 read the four tensor-memory lane quarters");
+  static_assert(NT == 512, "warps 4-15 read the four tensor-memory lane quarters, three each");
   constexpr int NW = NT / 32;
   const int ld = purify_ld(n), n16 = purify_n16(n);
   const int64_t part = (int64_t)n16 * ld;  // floats of one TF32 part (hi or lo)
@@ -112,7 +113,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf + b, 1);
-      mbar_init(acce + b, 4);
+      mbar_init(acce + b, 12);
     }
     mbar_init(drain, 1);
     mbar_fence_init();
@@ -208,9 +209,11 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
           ++mma_tiles;
         }
       }
-    } else if (warp >= 4 && warp < 8) {
-      // ---- epilogue: one thread per tile row (tensor-memory lane 32 (warp & 3) + lane) ----
+    } else if (warp >= 4) {
+      // ---- epilogue: warps 4-15, one thread per tile row (tensor-memory lane 32 (warp & 3) +
+      // lane), three warps per lane quarter, each taking a third of the 16-column chunks ----
       const int quad = warp & 3;
+      const int part = (warp - 4) >> 2;  // 0, 1, 2
       const int lr = 32 * quad + lane;
       for (int t = 0; t < T && !s_abort; ++t) {
         int I, J;
@@ -225,7 +228,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
         const int64_t row = (int64_t)r * ld;
         const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(b * kTfBM);
 #pragma unroll 1
-        for (int c0 = 0; c0 < kTfBM; c0 += 16) {
+        for (int c0 = 16 * part; c0 < kTfBM; c0 += 48) {
           uint32_t v[16];
           tmem_ld16(taddr + (uint32_t)c0, v);  // every lane: the load is warp-collective
           const int cb = J * kTfBM + c0;
