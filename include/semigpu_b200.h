@@ -89,6 +89,15 @@ int sgb_ctx_set_density_solver(sgb_ctx *ctx, int solver);
  * large-molecule class); semigpu_b200/autotune.py picks them by timing. */
 int sgb_size_classes(int *count, int *nao_max, int *threads, int max_count);
 int sgb_ctx_set_class_threads(sgb_ctx *ctx, int count, const int *threads);
+/* Tile configurations of the whole-GPU FP64 purification (one large molecule, sgb_scf above
+ * nao 160; no counterpart in the reference): *count configurations, configuration k has
+ * bm[k] x bm[k] tiles, warps[k] warps per CTA, kblocks[k] k-blocks of 16 doubles per TMA ring
+ * stage and stages[k] stages (arrays of max_count entries; any may be NULL).
+ * sgb_ctx_set_grid_config fixes the configuration for this context's single-molecule SCF runs
+ * (-1, the default: chosen by size -- the largest tile that gives every SM work);
+ * semigpu_b200/autotune.py tune_grid picks one by timing an SCF step. */
+int sgb_grid_configs(int *count, int *bm, int *warps, int *kblocks, int *stages, int max_count);
+int sgb_ctx_set_grid_config(sgb_ctx *ctx, int config);
 /* Caps the batched launches of this context at share x (number of SMs) CTAs' worth of SMs
  * (0 < share <= 1; 1 = the whole GPU, the default).  No counterpart in the reference; a
  * server running several contexts side by side uses it so that one context's persistent

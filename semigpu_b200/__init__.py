@@ -44,6 +44,8 @@ SIGNATURES = {
     "sgb_ctx_set_sm_share": (ctypes.c_int, [_VP, ctypes.c_double]),
     "sgb_ctx_set_diis": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_ctx_set_damping": (ctypes.c_int, [_VP, ctypes.c_double]),
+    "sgb_grid_configs": (ctypes.c_int, [_I, _I, _I, _I, _I, ctypes.c_int]),
+    "sgb_ctx_set_grid_config": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_ctx_set_limits": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_longlong]),
     "sgb_diag_barrier_timeout": (ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_longlong, _I]),
@@ -131,6 +133,17 @@ def size_classes() -> list[tuple[int, int]]:
     return [(int(a), int(b)) for a, b in zip(nmax, thr)]
 
 
+def grid_configs() -> list[dict]:
+    """Tile configurations of the whole-GPU purification: tile rows, warps, k-blocks per ring
+    stage, stages (index = the value for Context.set_grid_config)."""
+    n = ctypes.c_int()
+    lib().sgb_grid_configs(ctypes.byref(n), None, None, None, None, 0)
+    a = [np.zeros(n.value, np.int32) for _ in range(4)]
+    lib().sgb_grid_configs(ctypes.byref(n), *(_i(x) for x in a), n.value)
+    return [{"bm": int(a[0][k]), "warps": int(a[1][k]), "kblocks": int(a[2][k]),
+             "stages": int(a[3][k])} for k in range(n.value)]
+
+
 def mndo_parameters(z: int) -> np.ndarray:
     """The engine's MNDO parameters of element z (order of the SGB_P_* indices)."""
     out = np.zeros(18)
@@ -190,6 +203,11 @@ class Context:
         self.check(lib().sgb_electronic_energy(self.h, n, _d(H), _d(F), _d(P), ctypes.byref(e)),
                    "sgb_electronic_energy")
         return e.value
+
+    def set_grid_config(self, config: int):
+        """Tile configuration of the whole-GPU purification (index into grid_configs(); -1 =
+        chosen by size)."""
+        self.check(lib().sgb_ctx_set_grid_config(self.h, int(config)), "set_grid_config")
 
     def set_damping(self, factor: float):
         """Density damping 0 <= factor < 1 (0 = off): P = (1 - f) P_new + f P_old each step."""

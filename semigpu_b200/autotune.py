@@ -1,4 +1,5 @@
-"""Autotuner of the batched launch: picks the CTA size of each nao size class by timing.
+"""Autotuners: the CTA size of each nao size class of the batched launch (`tune`), and the tile
+configuration of the whole-GPU purification for one large molecule (`tune_grid`), by timing.
 
 Each size class of `k_batch_scf` can run with CTAs of 128 (classes up to nao 64), 256 or 512
 threads; smaller CTAs fit more molecules per SM, larger ones give each molecule more warps for
@@ -94,3 +95,40 @@ def main(argv=None):
 
 if __name__ == "__main__":
     main()
+
+
+def tune_grid(ctx: Context, mol, repeats: int = 2, steps: int = 1, tol: float = 1e-6,
+              min_gain: float = 0.01) -> dict:
+    """Tile configuration of the whole-GPU purification for molecules like `mol` (a geometry
+    above nao 160): times `steps` SCF steps of `mol` with every configuration of
+    `grid_configs()` (the automatic choice first), keeps the fastest if it beats the automatic
+    one by more than `min_gain`, and applies it to `ctx` (Context.set_grid_config).  Returns
+    {"config": index or -1, "ms": ..., "auto_ms": ..., "trials": [(config, ms), ...]}."""
+    import time
+
+    from . import Molecule, grid_configs
+
+    def run(cfg):
+        ctx.set_grid_config(cfg)
+        best = float("inf")
+        for _ in range(repeats + 1):  # the first run also compiles nothing but warms the arenas
+            m = Molecule(ctx, mol.Z, mol.xyz)
+            m.set_path(2)  # PATH_GRID
+            m.two_center()
+            m.hcore()
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            m.scf(tol=tol, max_iter=steps)
+            best = min(best, time.perf_counter() - t0)
+            m.close()
+        return 1e3 * best
+
+    trials = [(-1, run(-1))]
+    for k in range(len(grid_configs())):
+        trials.append((k, run(k)))
+    auto_ms = trials[0][1]
+    cfg, ms = min(trials[1:], key=lambda t: t[1])
+    if not ms < auto_ms * (1.0 - min_gain):
+        cfg, ms = -1, auto_ms
+    ctx.set_grid_config(cfg)
+    return {"config": cfg, "ms": ms, "auto_ms": auto_ms, "trials": trials}

@@ -90,6 +90,7 @@ struct sgb_ctx {
   int max_sweeps = 0;          // Jacobi sweeps per eigensolve (0: the path's default)
   long long wait_spins = -1;   // polls of a bounded device wait (< 0: the default bound)
   double damping = 0.0;        // density damping factor (0: off)
+  int grid_config = -1;        // tile configuration of the whole-GPU purification (-1: by size)
   // Timing events for batches, created with the context and recycled: cudaEventCreate waits
   // for the kernels running on the device, which would stall a batch built while another
   // context's long launch runs.
@@ -970,17 +971,29 @@ int grid_lanczos_bounds(sgb_ctx* ctx, sgb_mol* mol, double* lohi) {
 
 // Tile configuration of the device purification loop for order n: the largest tile that
 // still gives every SM work (two tiles per SM for the 128 x 128 tile, one for 64 x 64).
-// SGB_GRID_TILE=32, 64 or 128 overrides the choice (for tile-size sweeps).
-int gp_tile(int n, int num_sms) {
-  if (const char* env = getenv("SGB_GRID_TILE")) {
-    const int t = atoi(env);
-    if (t == GpLarge::BM || t == GpMid::BM || t == GpSmall::BM) return t;
-  }
+// The tile configurations of the whole-GPU FP64 purification (sgb_grid_configs): tile rows,
+// warps, k-blocks per ring stage, stages.
+struct GridConfigInfo {
+  int bm, warps, kb, stages;
+};
+constexpr GridConfigInfo kGridConfigs[] = {
+    {GpLarge::BM, GpLarge::WARPS, GpLarge::KB, GpLarge::STAGES},
+    {GpLargeAlt1::BM, GpLargeAlt1::WARPS, GpLargeAlt1::KB, GpLargeAlt1::STAGES},
+    {GpLargeAlt2::BM, GpLargeAlt2::WARPS, GpLargeAlt2::KB, GpLargeAlt2::STAGES},
+    {GpMid::BM, GpMid::WARPS, GpMid::KB, GpMid::STAGES},
+    {GpSmall::BM, GpSmall::WARPS, GpSmall::KB, GpSmall::STAGES}};
+constexpr int kNumGridConfigs = 5;
+
+// Configuration index for order n: the context's choice, else the largest tile that still gives
+// every SM work (two tiles per SM for the 128 x 128 tile, one for 64 x 64).
+int gp_config(const sgb_ctx* ctx, int n) {
+  if (ctx->grid_config >= 0) return ctx->grid_config;
   auto tiles = [](int n, int bm) { const int64_t t = (n + bm - 1) / bm; return t * (t + 1) / 2; };
-  if (tiles(n, GpLarge::BM) >= 2LL * num_sms) return GpLarge::BM;
-  if (tiles(n, GpMid::BM) >= num_sms) return GpMid::BM;
-  return GpSmall::BM;
+  if (tiles(n, GpLarge::BM) >= 2LL * ctx->num_sms) return 0;
+  if (tiles(n, GpMid::BM) >= ctx->num_sms) return 3;
+  return 4;
 }
+
 
 // Dynamic shared memory cap of each configuration, once per device (cudaFuncSetAttribute
 // waits for running kernels, so this runs at context creation).
@@ -1148,7 +1161,8 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
     int rc = grid_lanczos_bounds(ctx, mol, sc + 2);
     if (rc) return rc;
   }
-  const int bm = gp_tile(n, ctx->num_sms);
+  const int cfg = gp_config(ctx, n);
+  const int bm = kGridConfigs[cfg].bm;
   const int np = (n + bm - 1) / bm * bm;
   const int nbp = grid_blocks(ctx, (int64_t)np * np);
   *products = -1;
@@ -1180,13 +1194,13 @@ int grid_purify(sgb_ctx* ctx, sgb_mol* mol, bool mixed, int* products) {
   CUDA_TRY(ctx, cudaGetLastError());
   int prod = -1;
   double* Xf = nullptr;
-  const char* var = getenv("SGB_GRID_VARIANT");  // alternatives of the 128 tile (sweeps)
-  const int vsel = var ? atoi(var) : 0;
-  if (bm == GpLarge::BM && vsel == 1) rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
-  else if (bm == GpLarge::BM && vsel == 2) rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
-  else if (bm == GpLarge::BM) rc = gp_launch<GpLarge>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
-  else if (bm == GpMid::BM) rc = gp_launch<GpMid>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
-  else rc = gp_launch<GpSmall>(ctx, mol, np, it0, swap, mixed, &prod, &Xf);
+  switch (cfg) {
+    case 0: rc = gp_launch<GpLarge>(ctx, mol, np, it0, swap, mixed, &prod, &Xf); break;
+    case 1: rc = gp_launch<GpLargeAlt1>(ctx, mol, np, it0, swap, mixed, &prod, &Xf); break;
+    case 2: rc = gp_launch<GpLargeAlt2>(ctx, mol, np, it0, swap, mixed, &prod, &Xf); break;
+    case 3: rc = gp_launch<GpMid>(ctx, mol, np, it0, swap, mixed, &prod, &Xf); break;
+    default: rc = gp_launch<GpSmall>(ctx, mol, np, it0, swap, mixed, &prod, &Xf); break;
+  }
   if (rc) return rc;
   if (prod >= 0) {
     k_gp_density<<<grid_blocks(ctx, tri(n)), kGridThreads, 0, st>>>(n, np, Xf, v.P, ctx->damping);
@@ -1601,6 +1615,23 @@ int sgb_ctx_set_class_threads(sgb_ctx* ctx, int count, const int* threads) {
 int sgb_ctx_set_diis(sgb_ctx* ctx, int depth) {
   if (!ctx || depth < 0 || depth > 8 || depth == 1) return SGB_E_ARG;
   ctx->diis = depth;
+  return SGB_OK;
+}
+
+int sgb_grid_configs(int* count, int* bm, int* warps, int* kblocks, int* stages, int max_count) {
+  if (count) *count = kNumGridConfigs;
+  for (int k = 0; k < kNumGridConfigs && k < max_count; ++k) {
+    if (bm) bm[k] = kGridConfigs[k].bm;
+    if (warps) warps[k] = kGridConfigs[k].warps;
+    if (kblocks) kblocks[k] = kGridConfigs[k].kb;
+    if (stages) stages[k] = kGridConfigs[k].stages;
+  }
+  return SGB_OK;
+}
+
+int sgb_ctx_set_grid_config(sgb_ctx* ctx, int config) {
+  if (!ctx || config < -1 || config >= kNumGridConfigs) return SGB_E_ARG;
+  ctx->grid_config = config;
   return SGB_OK;
 }
 

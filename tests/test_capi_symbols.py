@@ -53,3 +53,14 @@ def test_size_classes_cover_the_batched_range():
     bounds = [n for n, _ in cls]
     assert bounds == sorted(bounds) and bounds[0] == 32 and 1024 in bounds
     assert {t for _, t in cls} <= {128, 256, 512}
+
+
+def test_grid_configs_without_gpu():
+    """The whole-GPU purification's tile configurations, listed without a device: the default
+    (index 0) is the 128 x 128 tile; every tile is a whole number of 8 x 8 DMMA fragments."""
+    import semigpu_b200 as sg
+
+    cfgs = sg.grid_configs()
+    assert len(cfgs) == 5 and cfgs[0]["bm"] == 128
+    assert {c["bm"] for c in cfgs} == {32, 64, 128}
+    assert all(c["bm"] % 8 == 0 and 1 <= c["stages"] <= 8 and c["warps"] in (4, 8, 16) for c in cfgs)

@@ -41,3 +41,35 @@ def test_autotuner_returns_a_valid_choice():
         assert np.all(r["converged"])
     finally:
         ctx.close()
+
+
+def test_every_grid_config_gives_the_same_scf():
+    """One molecule on the whole GPU with each tile configuration of the purification loop:
+    the same steps and energy (the products differ only in summation order)."""
+    mol = geo.alkane(50, np.random.default_rng(6))  # nao 302
+    ctx = sg.Context(0)
+    try:
+        out = []
+        for k in [-1] + list(range(len(sg.grid_configs()))):
+            ctx.set_grid_config(k)
+            out.append(sg.Molecule.from_geometry(ctx, mol).run(tol=1e-6))
+        with pytest.raises(sg.SGBError):
+            ctx.set_grid_config(len(sg.grid_configs()))
+    finally:
+        ctx.close()
+    for r in out[1:]:
+        assert r["status"] == 0 and r["n_iter"] == out[0]["n_iter"]
+        assert abs(r["E_tot"] - out[0]["E_tot"]) < 1e-8
+
+
+def test_grid_autotuner_returns_a_valid_choice():
+    mol = geo.alkane(60, np.random.default_rng(7))  # nao 362
+    ctx = sg.Context(0)
+    try:
+        res = autotune.tune_grid(ctx, mol, repeats=1)
+        assert res["config"] in [-1] + list(range(len(sg.grid_configs())))
+        assert res["ms"] <= res["auto_ms"]
+        r = sg.Molecule.from_geometry(ctx, mol).run(tol=1e-6)
+        assert r["converged"] and r["status"] == 0
+    finally:
+        ctx.close()
