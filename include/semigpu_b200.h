@@ -235,6 +235,14 @@ int sgb_batch_results(sgb_ctx *ctx, sgb_batch *b, double *e_el, double *e_cc, in
 int sgb_run_molecules(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, const double *xyz,
                       double tol, int max_iter, double *e_el, double *e_cc, int *n_iter,
                       int *converged, int *status);
+/* Geometry gradient of the total energy, dE_tot/dxyz in eV/Angstrom (natoms*3 values, the
+ * order of xyz), by central differences: the molecule and its 6 natoms copies displaced by
+ * +/- step Angstrom along each coordinate run as one batch (one CTA per geometry, nao <= 1024);
+ * *e_tot (may be NULL) receives the undisplaced total energy.  The SCF tolerance sets the
+ * noise: about tol / step (use tol near 1e-9 eV with step 1e-4 Angstrom).  No counterpart in
+ * the reference, whose README lists a geometry optimizer as future work (README.md:110). */
+int sgb_gradient(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, double tol,
+                 int max_iter, double step, double *e_tot, double *grad);
 /* Kernel launches one sgb_batch_run makes (one persistent launch per occupied size class). */
 int sgb_batch_launches(const sgb_batch *b, int *launches);
 /* Device-time of the last sgb_batch_run in milliseconds (CUDA events on the context stream). */

@@ -72,6 +72,8 @@ SIGNATURES = {
     "sgb_run_molecules": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.c_double,
                                          ctypes.c_int, _D, _D, _I, _I, _I]),
     "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "sgb_gradient": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.c_double, ctypes.c_int,
+                                    ctypes.c_double, _D, _D]),
     "sgb_batch_launches": (ctypes.c_int, [_VP, _I]),
     "sgb_scf_noalloc": (ctypes.c_int, [ctypes.c_int, _I, _D, ctypes.c_double, ctypes.c_int, _VP,
                                        _D, _D, _I, _I, _I]),
@@ -440,3 +442,61 @@ def run_molecules(ctx: Context, mols, tol: float = 1e-6, max_iter: int = 100) ->
                                       _d(eel), _d(ecc), _i(it), _i(cv), _i(st)), "sgb_run_molecules")
     return {"E_el": eel, "E_cc": ecc, "E_tot": eel + ecc, "n_iter": it,
             "converged": cv.astype(bool), "status": st}
+
+
+def gradient(ctx: Context, mol, tol: float = 1e-9, max_iter: int = 200, step: float = 1e-4):
+    """(E_tot, dE_tot/dxyz in eV/Angstrom, shape (natoms, 3)) by central differences, the 6N
+    displaced geometries in one batched launch (sgb_gradient)."""
+    Z = np.ascontiguousarray(mol.Z, np.int32)
+    xyz = np.ascontiguousarray(mol.xyz, np.float64).reshape(-1)
+    g = np.zeros_like(xyz)
+    e = ctypes.c_double()
+    ctx.check(lib().sgb_gradient(ctx.h, len(Z), _i(Z), _d(xyz), tol, max_iter, step,
+                                 ctypes.byref(e), _d(g)), "sgb_gradient")
+    return e.value, g.reshape(-1, 3)
+
+
+def optimize(ctx, mol, gtol: float = 0.02, max_steps: int = 50, tol: float = 1e-9,
+             step: float = 1e-4, max_move: float = 0.2, energy_gradient=None):
+    """Geometry optimisation (BFGS on the Cartesian coordinates, moves capped at max_move
+    Angstrom, backtracking when the energy rises) with the finite-difference gradients of
+    `gradient`; stops when every gradient component is below gtol eV/Angstrom.  A caller may
+    pass energy_gradient(molecule) -> (E_tot, gradient) instead of a context.  Returns
+    (optimised geometry, E_tot, max |gradient|, steps)."""
+    x = np.ascontiguousarray(mol.xyz, np.float64).reshape(-1).copy()
+    n = x.size
+    if energy_gradient is None:
+        def energy_gradient(m):
+            return gradient(ctx, m, tol=tol, step=step)
+
+    def eg(xx):
+        return energy_gradient(geometry.Molecule(mol.Z, xx.reshape(-1, 3)))
+
+    e, g = eg(x)
+    g = g.reshape(-1)
+    Hinv = np.eye(n) / 50.0  # eV / Angstrom^2 scale of bond stretches
+    it = 0
+    for it in range(1, max_steps + 1):
+        if np.max(np.abs(g)) < gtol:
+            it -= 1
+            break
+        p = -Hinv @ g
+        big = np.max(np.abs(p))
+        if big > max_move:
+            p *= max_move / big
+        alpha = 1.0
+        while True:
+            xn = x + alpha * p
+            en, gn = eg(xn)
+            gn = gn.reshape(-1)
+            if en <= e + 1e-4 * alpha * float(g @ p) or alpha < 1e-3:
+                break
+            alpha *= 0.5
+        s_, y = xn - x, gn - g
+        sy = float(s_ @ y)
+        if sy > 1e-10:  # BFGS update of the inverse Hessian
+            rho = 1.0 / sy
+            I = np.eye(n)
+            Hinv = (I - rho * np.outer(s_, y)) @ Hinv @ (I - rho * np.outer(y, s_)) + rho * np.outer(s_, s_)
+        x, e, g = xn, en, gn
+    return geometry.Molecule(mol.Z, x.reshape(-1, 3)), e, float(np.max(np.abs(g))), it

@@ -2043,6 +2043,44 @@ int sgb_batch_device_coordinates(sgb_batch* b, void** dptr) {
   return SGB_OK;
 }
 
+int sgb_gradient(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, double tol, int max_iter,
+                 double step, double* e_tot, double* grad) {
+  if (!ctx || natoms <= 0 || !Z || !xyz || !grad || !(step > 0.0) || !(tol >= 0.0) || max_iter < 1)
+    return SGB_E_ARG;
+  // the molecule and its 6 natoms displaced copies (+/- step along each coordinate), one batch
+  const int nmol = 1 + 6 * natoms;
+  const int64_t per = 3 * (int64_t)natoms;
+  std::vector<int> na(nmol, natoms), zz((size_t)nmol * natoms);
+  std::vector<double> xx((size_t)nmol * per);
+  for (int m = 0; m < nmol; ++m) {
+    std::copy(Z, Z + natoms, zz.begin() + (size_t)m * natoms);
+    std::copy(xyz, xyz + per, xx.begin() + (size_t)m * per);
+    if (m > 0) {
+      const int64_t c = (m - 1) / 2;  // coordinate 3 atom + axis
+      xx[(size_t)m * per + c] += (m - 1) % 2 == 0 ? step : -step;
+    }
+  }
+  sgb_batch* b = nullptr;
+  int rc = build_batch(ctx, nmol, na.data(), zz.data(), xx.data(), 0, &b);
+  if (rc) return rc;
+  std::vector<double> eel(nmol), ecc(nmol);
+  std::vector<int> st(nmol), cv(nmol);
+  rc = sgb_batch_run(ctx, b, tol, max_iter);
+  if (!rc) rc = sgb_batch_results(ctx, b, eel.data(), ecc.data(), nullptr, cv.data(), st.data());
+  free_batch(b);
+  if (rc) return rc;
+  for (int m = 0; m < nmol; ++m) {
+    if (st[m] != MOL_OK) return st[m] == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN;
+    if (!cv[m]) return fail(ctx, SGB_E_EIG, "gradient: SCF of geometry %d did not converge", m);
+  }
+  if (e_tot) *e_tot = eel[0] + ecc[0];
+  for (int64_t c = 0; c < per; ++c) {
+    const int p = 1 + 2 * (int)c, q = p + 1;
+    grad[c] = ((eel[p] + ecc[p]) - (eel[q] + ecc[q])) / (2.0 * step);
+  }
+  return SGB_OK;
+}
+
 int sgb_run_molecules(sgb_ctx* ctx, int nmol, const int* natoms, const int* Z, const double* xyz,
                       double tol, int max_iter, double* e_el, double* e_cc, int* n_iter,
                       int* converged, int* status) {
