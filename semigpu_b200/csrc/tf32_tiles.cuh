@@ -52,20 +52,23 @@ constexpr int kBpTfStages = 2;  // 2 x 64 KB
 constexpr size_t kBpRingBytes =
     1024 + (kBpRingFp64 > (size_t)kBpTfStages * kTfStageBytes ? kBpRingFp64
                                                                : (size_t)kBpTfStages * kTfStageBytes) +
-    256;
+    256;  // alignment, the stages, the barriers
 // For these orders the FP32 phase's idempotency floor is near 1e-4 (n eigenvalues with FP32-level
 // errors), so it hands over to FP64 at 1e-3, as the whole-GPU form does.
 constexpr double kBpTf32Switch = 1e-3;
 
 // The mixed form of block_purify_tiles for one CTA of 512 threads: X_0 from F in FP64 (slot X),
-// split into TF32 hi / lo in slot Y (set 1; hi then lo, row stride n16 + 8 floats each, so a
-// set fills one slot), then products on the tensor cores while tr(X - X^2) >= kBpTf32Switch --
-// warp 0 loads, warp 1 issues the MMAs into one of two 128-column accumulators, warps 4-15
-// (one thread per tile row, three warps per row) read the accumulator and write the new hi / lo
-// into the other set
-// -- then X widened to FP64 into the slot the last set does not hold and bp_fp64_loop finishes.
-// maps: [0] X slot FP64, [1] Y slot FP64, [2] / [3] hi / lo of set 0 (slot X), [4] / [5] hi / lo
-// of set 1 (slot Y); 128-row boxes of 32 floats for the FP32 ones.
+// rounded to FP32 into slot Y (set 1: one FP32 matrix, row stride n16 + 8 floats), then products
+// on the tensor cores while tr(X - X^2) >= kBpTf32Switch -- warp 0 loads each k-block's two
+// panels (one on a diagonal tile) by TMA into the hi parts of a ring stage, warps 2-3 split them
+// in place into hi and lo (same swizzled offsets in the two parts), warp 1 issues the three MMAs
+// per k-slice into one of two 128-column accumulators, warps 4-15 (one thread per tile row,
+// three warps per row) read the accumulator and write the new X into the other set -- then X is
+// widened to FP64 into the slot the last set does not hold and bp_fp64_loop finishes.  Keeping
+// X in FP32 and splitting on chip halves the panel bytes each tile reads from memory (hi and lo
+// both held in memory before): with every SM streaming its own molecule's panels this phase is
+// bound by DRAM.  maps: [0] X slot FP64, [1] Y slot FP64, [2] set 0 FP32 (slot X), [4] set 1
+// FP32 (slot Y), 128-row boxes of 32 floats; [3] and [5] are not used here.
 template <int NT>
 __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int nocc, double* X,
                                                  double* Y, const CUtensorMap* maps,
@@ -74,24 +77,20 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
   static_assert(NT == 512, "warps 4-15 read the four tensor-memory lane quarters, three each");
   constexpr int NW = NT / 32;
   const int ld = purify_ld(n), n16 = purify_n16(n);
-  const int64_t part = (int64_t)n16 * ld;  // floats of one TF32 part (hi or lo)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   __shared__ volatile int s_abort;
   __shared__ uint32_t s_tmem;
   double t1, t2;
   purify_init<NT>(F, n, X, ld, lz, red, t1, t2);
   float* hs[2] = {reinterpret_cast<float*>(X), reinterpret_cast<float*>(Y)};
-  {  // X_0 (FP64) -> set 1 (hi, lo) with its sums
+  {  // X_0 (FP64) -> set 1 (FP32) with its sums
     double s1 = 0.0, s2 = 0.0;
     float* H = hs[1];
-    float* L = H + part;
     for (int64_t t = threadIdx.x; t < (int64_t)n16 * n16; t += NT) {
       const int r = (int)(t / n16), c = (int)(t - (int64_t)r * n16);
-      float h, l;
-      tf32_split((float)X[(int64_t)r * ld + c], h, l);
-      H[(int64_t)r * ld + c] = h;
-      L[(int64_t)r * ld + c] = l;
-      const double x = (double)h + (double)l;
+      const float v = (float)X[(int64_t)r * ld + c];
+      H[(int64_t)r * ld + c] = v;
+      const double x = (double)v;
       if (r == c) s1 += x;
       s2 = fma(x, x, s2);
     }
@@ -101,15 +100,20 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
   }
   unsigned char* tiles = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(ring_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kBpTfStages * kTfStageBytes);
+  // the barriers sit past the stages of both this ring and the FP64 ring that follows
+  // (bp_fp64_loop puts its own right after its stages), so the two never share an address
+  static_assert(kBpTfStages * kTfStageBytes >= kBpRingFp64, "the FP64 ring is not larger");
+  uint64_t* full = reinterpret_cast<uint64_t*>(tiles + kBpTfStages * kTfStageBytes + 128);
   uint64_t* empty = full + kBpTfStages;
-  uint64_t* accf = empty + kBpTfStages;
+  uint64_t* ready = empty + kBpTfStages;
+  uint64_t* accf = ready + kBpTfStages;
   uint64_t* acce = accf + 2;
   uint64_t* drain = acce + 2;
   if (threadIdx.x == 0) {
     for (int s = 0; s < kBpTfStages; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
+      mbar_init(ready + s, 2);  // the two splitting warps
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(accf + b, 1);
@@ -131,7 +135,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
   const int nt = (n16 + kTfBM - 1) / kTfBM, T = nt * (nt + 1) / 2;
   const int kblocks = (n16 + kTfK - 1) / kTfK;
   const uint32_t idesc = umma_idesc_tf32(kTfBM, kTfBM);
-  long long issued = 0, consumed = 0, mma_tiles = 0, epi_tiles = 0;
+  long long issued = 0, split = 0, consumed = 0, mma_tiles = 0, epi_tiles = 0;
   int cur = 1, it = 0;
   bool ok = true;
   for (;; ++it) {
@@ -142,12 +146,9 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
     if (t1 - t2 < kBpTf32Switch) break;
     const double n_o = (double)nocc;
     const bool sq = fabs(t2 - n_o) < fabs(2.0 * t1 - t2 - n_o);
-    const CUtensorMap* mh = maps + 2 + 2 * cur;
-    const CUtensorMap* ml = mh + 1;
-    const float* Xh = hs[cur];
-    const float* Xl = Xh + part;
-    float* Yh = hs[cur ^ 1];
-    float* Yl = Yh + part;
+    const CUtensorMap* mx = maps + 2 + 2 * cur;
+    const float* Xs = hs[cur];
+    float* Ys = hs[cur ^ 1];
     double s1 = 0.0, s2 = 0.0;
     if (warp == 0) {
       if (lane == 0) {  // ---- loader ----
@@ -162,18 +163,54 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
               break;
             }
             unsigned char* st = tiles + s * kTfStageBytes;
-            mbar_arrive_expect_tx(full + s, kTfStageBytes);
-            tma_load_2d(st, mh, kb * kTfK, I * kTfBM, full + s);
-            tma_load_2d(st + kTfBox, ml, kb * kTfK, I * kTfBM, full + s);
-            tma_load_2d(st + 2 * kTfBox, mh, kb * kTfK, J * kTfBM, full + s);
-            tma_load_2d(st + 3 * kTfBox, ml, kb * kTfK, J * kTfBM, full + s);
+            mbar_arrive_expect_tx(full + s, I == J ? kTfBox : 2 * kTfBox);
+            tma_load_2d(st, mx, kb * kTfK, I * kTfBM, full + s);
+            if (I != J) tma_load_2d(st + 2 * kTfBox, mx, kb * kTfK, J * kTfBM, full + s);
             ++issued;
           }
+        }
+      }
+    } else if (warp == 2 || warp == 3) {
+      // ---- split: each loaded FP32 part -> hi (in place) and lo (the next 16 KB) ----
+      const int tid = threadIdx.x - 64;
+      for (int t = 0; t < T && !s_abort; ++t) {
+        int I, J;
+        tri_inverse(t, I, J);
+        const int parts = I == J ? 1 : 2;
+        for (int kb = 0; kb < kblocks; ++kb) {
+          const int s = (int)(split % kBpTfStages);
+          if (!mbar_wait(full + s, (uint32_t)((split / kBpTfStages) & 1), spins)) {
+            s_abort = 1;
+            break;
+          }
+          unsigned char* st = tiles + s * kTfStageBytes;
+          for (int p = 0; p < parts; ++p) {
+            float4* hb = reinterpret_cast<float4*>(st + 2 * p * kTfBox);
+            float4* lb = reinterpret_cast<float4*>(st + (2 * p + 1) * kTfBox);
+#pragma unroll 4
+            for (int q = tid; q < kTfBox / 16; q += 64) {
+              const float4 v = hb[q];
+              float4 h, l;
+              tf32_split(v.x, h.x, l.x);
+              tf32_split(v.y, h.y, l.y);
+              tf32_split(v.z, h.z, l.z);
+              tf32_split(v.w, h.w, l.w);
+              hb[q] = h;
+              lb[q] = l;
+            }
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // read by the MMAs
+          __syncwarp();
+          if (lane == 0) mbar_arrive(ready + s);
+          ++split;
         }
       }
     } else if (warp == 1) {
       if (lane == 0) {  // ---- MMA issue ----
         for (int t = 0; t < T && !s_abort; ++t) {
+          int I, J;
+          tri_inverse(t, I, J);
+          const uint32_t boff = I == J ? 0u : 2u * kTfBox;  // a diagonal tile squares its panel
           const int b = (int)(mma_tiles & 1);
           const long long use = mma_tiles >> 1;
           if (use >= 1 && !mbar_wait(acce + b, (uint32_t)((use - 1) & 1), spins)) {
@@ -184,7 +221,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
           const uint32_t d = tmem + (uint32_t)(b * kTfBM);
           for (int kb = 0; kb < kblocks; ++kb) {
             const int s = (int)(consumed % kBpTfStages);
-            if (!mbar_wait(full + s, (uint32_t)((consumed / kBpTfStages) & 1), spins)) {
+            if (!mbar_wait(ready + s, (uint32_t)((consumed / kBpTfStages) & 1), spins)) {
               s_abort = 1;
               break;
             }
@@ -195,8 +232,8 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
               const uint32_t off = (uint32_t)ks * 32;
               const uint64_t ah = umma_desc_sw128(base + off);
               const uint64_t al = umma_desc_sw128(base + kTfBox + off);
-              const uint64_t bh = umma_desc_sw128(base + 2 * kTfBox + off);
-              const uint64_t bl = umma_desc_sw128(base + 3 * kTfBox + off);
+              const uint64_t bh = umma_desc_sw128(base + boff + off);
+              const uint64_t bl = umma_desc_sw128(base + boff + kTfBox + off);
               umma_tf32(d, ah, bh, idesc, (kb | ks) ? 1u : 0u);
               umma_tf32(d, ah, bl, idesc, 1u);
               umma_tf32(d, al, bh, idesc, 1u);
@@ -239,26 +276,31 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
             // the old X only enters the 2X - X^2 branch
             float old[4] = {0.0f, 0.0f, 0.0f, 0.0f};
             if (!sq) {
-              const float4 oh = __ldcg(reinterpret_cast<const float4*>(Xh + row + c));
-              const float4 ol = __ldcg(reinterpret_cast<const float4*>(Xl + row + c));
-              old[0] = oh.x + ol.x; old[1] = oh.y + ol.y; old[2] = oh.z + ol.z; old[3] = oh.w + ol.w;
+              const float4 o = __ldcg(reinterpret_cast<const float4*>(Xs + row + c));
+              old[0] = o.x; old[1] = o.y; old[2] = o.z; old[3] = o.w;
             }
+            float xn[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const float d2 = __uint_as_float(v[4 * g4 + e]);
+              xn[e] = sq ? d2 : fmaf(2.0f, old[e], -d2);
+            }
+            // the thread's own row: one 16-byte store when the four columns are all at or below
+            // the diagonal (a lane per row, so 4-byte stores would each take a sector); the
+            // mirror column: lanes hold consecutive rows, so those stores coalesce
+            if (r >= c + 3)
+              __stcg(reinterpret_cast<float4*>(Ys + row + c), make_float4(xn[0], xn[1], xn[2], xn[3]));
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               const int ce = c + e;
               if (r < ce) continue;
-              const float d2 = __uint_as_float(v[4 * g4 + e]);
-              float h, l;
-              tf32_split(sq ? d2 : fmaf(2.0f, old[e], -d2), h, l);
-              __stcg(Yh + row + ce, h);
-              __stcg(Yl + row + ce, l);
-              const double x = (double)h + (double)l;
+              if (r < c + 3) __stcg(Ys + row + ce, xn[e]);
+              const double x = (double)xn[e];
               if (r == ce) {
                 s1 += x;
                 s2 = fma(x, x, s2);
               } else {
-                __stcg(Yh + (int64_t)ce * ld + r, h);
-                __stcg(Yl + (int64_t)ce * ld + r, l);
+                __stcg(Ys + (int64_t)ce * ld + r, xn[e]);
                 s2 = fma(2.0 * x, x, s2);
               }
             }
@@ -302,6 +344,12 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
       umma_commit(drain);
       mbar_wait(drain, 0, kMbarSpins);
     }
+  } else if (warp == 0 && lane == 0) {
+    // the MMAs' last releases of the stages (tcgen05.commit arrivals nobody waited for): let
+    // them land before the barriers are invalidated
+    for (long long c = issued - kBpTfStages; c < issued; ++c)
+      if (c >= 0)
+        mbar_wait(empty + (int)(c % kBpTfStages), (uint32_t)((c / kBpTfStages) & 1), kMbarSpins);
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
@@ -313,6 +361,7 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
     for (int s = 0; s < kBpTfStages; ++s) {
       asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(full + s)));
       asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(empty + s)));
+      asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(ready + s)));
     }
     for (int b = 0; b < 2; ++b) {
       asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(accf + b)));
@@ -332,12 +381,11 @@ __device__ __noinline__ int block_purify_tiles32(const double* F, int n, int noc
   const CUtensorMap* mYd = cur ? maps + 1 : maps;
   {
     const float* H = hs[cur];
-    const float* L = H + part;
     double s1 = 0.0, s2 = 0.0;
     for (int64_t t = threadIdx.x; t < (int64_t)n16 * n16; t += NT) {
       const int r = (int)(t / n16), c = (int)(t - (int64_t)r * n16);
       const int64_t a = (int64_t)r * ld + c, bb = (int64_t)c * ld + r;
-      const double v = 0.5 * (((double)H[a] + (double)L[a]) + ((double)H[bb] + (double)L[bb]));
+      const double v = 0.5 * ((double)H[a] + (double)H[bb]);
       Xd[a] = v;
       if (r == c) s1 += v;
       s2 = fma(v, v, s2);

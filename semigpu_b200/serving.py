@@ -16,6 +16,9 @@ single-molecule grid path in the large-queue worker that picked them.
 
 `solver` picks how each SCF step gets the density (SOLVER_PURIFY, the FP64 default, or
 SOLVER_PURIFY_MIXED: TF32 tensor-core products with an FP64 finish, within 1e-4 eV of FP64).
+`diis` (depth 2..8, default off) turns on Pulay DIIS in every worker: fewer SCF steps per
+molecule, converged energies within the SCF tolerance of the plain loop's, step counts no longer
+the reference's.
 
 Latency of a request = completion time - arrival time (host clock); `stats()` reports p50/p99
 and throughput.  `replay()` drives an open-loop arrival schedule (e.g. Poisson) in real time.
@@ -36,15 +39,17 @@ CTA_MAX_NAO = 1024  # larger molecules take the grid path
 SMEM_MAX_NAO = 160  # above this a batched molecule also holds its work matrices in global memory
 
 
-def device_bytes(mol: Geometry) -> int:
+def device_bytes(mol: Geometry, diis: int = 0) -> int:
     """Device memory a molecule occupies inside a batch (integral blocks, Hcore/P/F packed,
     eigenvectors + F full square (+ the work matrices above nao 160), eigenvalues, atom
-    arrays)."""
+    arrays, and with DIIS of depth `diis` its history of 2 diis + 1 squares)."""
     heavy = int(np.count_nonzero(mol.Z > 1))
     light = mol.natoms - heavy
     nblk = 100 * heavy * (heavy + 1) // 2 + 10 * heavy * light + light * (light + 1) // 2
     n = mol.nao
     squares = 2 * n * n
+    if diis >= 2:
+        squares += (2 * diis + 1) * n * n + 128
     if n > SMEM_MAX_NAO:  # work matrices X and Y of purification, n16 x (n16 + 8) each
         n16 = (n + 15) // 16 * 16
         squares += max(n * n, 2 * n16 * (n16 + 8))
@@ -65,14 +70,16 @@ class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
                  batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
-                 big_sm_share: float = 0.85, solver: int | None = None):
+                 big_sm_share: float = 0.85, solver: int | None = None, diis: int = 0):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
         queue of molecules above nao 160 (at least one slot stays with the small queue); their
         launches together use at most big_sm_share of the SMs, so the persistent large-molecule
         launches (seconds) always leave SMs to the small ones.  solver: the density solver of
-        every worker context (None: the library default)."""
+        every worker context (None: the library default); diis: DIIS depth of every worker
+        context (0: off)."""
         self.solver = solver
+        self.diis = diis
         self.big_sm_share = big_sm_share
         self.tol, self.max_iter = tol, max_iter
         self.max_batch = max_batch
@@ -143,7 +150,7 @@ class Server:
         share."""
         out, used = [], 0
         while queue and len(out) < self.max_batch:
-            need = device_bytes(queue[0].mol)
+            need = device_bytes(queue[0].mol, self.diis)
             if out and used + need > self.slot_budget:
                 break
             used += need
@@ -158,6 +165,8 @@ class Server:
                 ctx = Context(self._device)
                 if self.solver is not None:
                     ctx.set_density_solver(self.solver)
+                if self.diis:
+                    ctx.set_diis(self.diis)
                 if big and self.big_slots:
                     ctx.set_sm_share(max(0.05, self.big_sm_share / self.big_slots))
                 # batches are built in a per-worker arena: no cudaMalloc/cudaFree per batch
@@ -249,6 +258,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mixed", action="store_true",
                     help="mixed precision (TF32 tensor-core products, FP64 finish)")
+    ap.add_argument("--diis", type=int, default=0, help="DIIS depth (2..8; 0: off)")
     args = ap.parse_args(argv)
     if args.workload == "c5":
         arrivals = geo.serving_c5(rate=args.rate, duration_s=args.duration, seed=args.seed)
@@ -263,7 +273,7 @@ def main(argv=None):
         arrivals = list(zip(times, geo.batch_c3(len(times), seed=args.seed)))
     srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)),
                  big_sm_share=args.big_share,
-                 solver=SOLVER_PURIFY_MIXED if args.mixed else SOLVER_PURIFY)
+                 solver=SOLVER_PURIFY_MIXED if args.mixed else SOLVER_PURIFY, diis=args.diis)
     try:
         srv.replay([(0.001 * i, m) for i, (_, m) in enumerate(arrivals[:40])])  # warm-up
         done = srv.replay(arrivals)
@@ -271,6 +281,7 @@ def main(argv=None):
         srv.close()
     out = {"workload": args.workload, "rate_per_s": args.rate, "duration_s": args.duration,
            "precision": "mixed" if args.mixed else "fp64", "big_share": args.big_share,
+           "diis": args.diis,
            "all": stats(done),
            "small": stats([r for r in done if r.mol.nao <= SMEM_MAX_NAO]),
            "large": stats([r for r in done if r.mol.nao > SMEM_MAX_NAO]),

@@ -82,6 +82,32 @@ def test_c100h202_in_batch_against_oracle(gpu_ctx, oracle_mod):
     assert abs(r["E_cc"][0] - o["E_cc"]) < 1e-6
 
 
+def test_large_fp64_tiles_without_fallback(oracle_mod):
+    """FP64 above nao 160 in the batch through both tile shapes of the TMA-staged loop (64 x 64
+    for nao 164 and 302, 128 x 128 for 202 and 452): the reference's energies and step counts,
+    with every step's density from purification (a failed purification would fall back to the
+    Jacobi eigensolve, which gives the same energies)."""
+    rng = np.random.default_rng(19)
+    mols = [geo.alkane(27, rng), geo.polyene(40, rng), geo.alkane(50, rng), geo.polyene(90, rng)]
+    assert [m.nao for m in mols] == [164, 202, 302, 452]
+    ctx = sg.Context(0)
+    try:
+        b = sg.Batch(ctx, mols)
+        b.set_profiling(True)
+        b.run(1e-6)
+        r = b.results()
+        sc = b.stage_cycles()
+        b.close()
+    finally:
+        ctx.close()
+    assert np.all(r["status"] == 0) and np.all(r["converged"])
+    assert np.all(sc[:, sg.Batch.STAGES.index("full_solves")] == 0)
+    for i, m in enumerate(mols):
+        o = oracle_mod.scf(m.Z, m.xyz, tol=1e-6)
+        assert r["n_iter"][i] == o["n_iter"], m.nao
+        assert abs(r["E_tot"][i] - o["E_tot"]) < 1e-6, (m.nao, r["E_tot"][i] - o["E_tot"])
+
+
 def test_large_mixed_tensor_core_against_oracle(oracle_mod):
     """Mixed form above nao 160 in the batch (one CTA per molecule): the TF32 tensor-core phase
     on TMA-staged hi / lo panels, then the FP64 tile loop; every molecule within 1e-4 eV of the
