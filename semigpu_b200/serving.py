@@ -70,7 +70,7 @@ class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
                  batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
-                 big_sm_share: float = 0.85, solver: int | None = None, diis: int = 0):
+                 big_sm_share: float = 0.95, solver: int | None = None, diis: int = 0):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
         queue of molecules above nao 160 (at least one slot stays with the small queue); their
@@ -222,15 +222,26 @@ class Server:
 
 
 def stats(done: list[Request]) -> dict:
-    """p50/p99 time-to-converged-energy (arrival -> result) and throughput."""
+    """p50/p99 time-to-converged-energy (arrival -> result) and throughput (requests over the
+    span from the first arrival to the last result, so the final drain counts against it).
+    Whether the load is sustained shows in p50_ms_by_arrival_quarter: the p50 latency of the
+    requests arriving in each quarter of the arrival span, flat when no backlog builds, and in
+    drain_ms, the time from the last arrival to the last result."""
     if not done:
         return {}
     lat = np.array([r.t_done - r.t_arrival for r in done])
-    t_first = min(r.t_arrival for r in done)
+    arr = np.array([r.t_arrival for r in done])
+    t_first, t_last_arrival = float(arr.min()), float(arr.max())
     t_last = max(r.t_done for r in done)
+    span = max(t_last_arrival - t_first, 1e-9)
+    quarter = np.minimum((4 * (arr - t_first) / span).astype(int), 3)
     return {"requests": len(done), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
             "p99_ms": 1e3 * float(np.percentile(lat, 99)),
             "molecules_per_s": len(done) / (t_last - t_first) if t_last > t_first else float("nan"),
+            "p50_ms_by_arrival_quarter": [
+                1e3 * float(np.percentile(lat[quarter == k], 50)) if np.any(quarter == k) else None
+                for k in range(4)],
+            "drain_ms": 1e3 * (t_last - t_last_arrival),
             "all_converged": bool(all(r.result.get("converged", False) for r in done))}
 
 
@@ -253,7 +264,7 @@ def main(argv=None):
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--big-slots", type=int, default=2)
     ap.add_argument("--hbm-gb", type=float, default=40.0)
-    ap.add_argument("--big-share", type=float, default=0.85,
+    ap.add_argument("--big-share", type=float, default=0.95,
                     help="fraction of the SMs the large-molecule workers' launches may use")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--mixed", action="store_true",

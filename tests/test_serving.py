@@ -144,3 +144,22 @@ def test_served_mixed_precision_within_tolerance_of_fp64():
             alone = sg.Molecule.from_geometry(ctx, mols[i]).run(tol=1e-6)
             assert done[i].result["n_iter"] == alone["n_iter"]
             assert abs(done[i].result["E_tot"] - alone["E_tot"]) < 1e-9
+
+
+def test_stats_latency_by_arrival_quarter():
+    """A backlog that grows shows as rising per-quarter p50; the drain is last result minus
+    last arrival."""
+    from semigpu_b200 import serving
+    from semigpu_b200.geometry import Molecule
+
+    m = Molecule([1, 1], [[0, 0, 0], [0.74, 0, 0]])
+    reqs = []
+    for i in range(40):
+        r = serving.Request(i, m, t_arrival=0.1 * i)
+        r.t_done = r.t_arrival + 0.01 * (1 + i // 10)  # 10, 20, 30, 40 ms by quarter
+        r.result = {"converged": True}
+        reqs.append(r)
+    st = serving.stats(reqs)
+    assert [round(v) for v in st["p50_ms_by_arrival_quarter"]] == [10, 20, 30, 40]
+    assert abs(st["drain_ms"] - 40.0) < 1e-6
+    assert st["requests"] == 40 and st["all_converged"]
