@@ -104,6 +104,64 @@ void Atom::PrintGeometry(const vector<Atom>& molecule) {
 // ---- ReadXYZFile (readxyzfile.cpp:27-133: count, comment line, symbol-or-number rows) ----
 ReadXYZFile::ReadXYZFile() : Natoms(0), open_without_problems(true) {}
 
+bool ReadXYZFile::GetFramesFromFile(string filename, vector<vector<Atom>>& frames,
+                                    vector<string>& comments) {
+  frames.clear();
+  comments.clear();
+  std::ifstream f(filename.c_str());
+  if (!f.good()) {
+    cout << "Error: File " << filename << " could not be opened...\n";
+    open_without_problems = false;
+    return false;
+  }
+  open_without_problems = false;
+  std::string line;
+  while (std::getline(f, line)) {
+    if (line.find_first_not_of(" \t\r") == std::string::npos) continue;  // between frames
+    std::stringstream head(line);
+    int n = 0;
+    if (!(head >> n) || n <= 0) {
+      cout << "Error: frame " << frames.size() << " of " << filename
+           << " does not start with an atom count" << endl;
+      return false;
+    }
+    std::string comment;
+    std::getline(f, comment);
+    vector<Atom> mol(n, Atom());
+    for (int i = 0; i < n; ++i) {
+      if (!std::getline(f, line)) {
+        cout << "Error: frame " << frames.size() << " of " << filename << " ends after " << i
+             << " of " << n << " atoms" << endl;
+        return false;
+      }
+      std::stringstream ls(line);
+      std::string tok;
+      double x = 0, y = 0, z = 0;
+      if (!(ls >> tok >> x >> y >> z)) {
+        cout << "Error: frame " << frames.size() << " of " << filename << ", atom " << i
+             << ": expected 'element x y z'" << endl;
+        return false;
+      }
+      if (tok.find_first_not_of("0123456789") == std::string::npos)
+        mol[i].setAtomNumber(atoi(tok.c_str()));
+      else
+        mol[i].setAtomSymbol(tok);
+      mol[i].setCoordinates(x, y, z);
+      if (!mol[i].statusData) {
+        cout << "Error: frame " << frames.size() << " of " << filename << ", atom " << i
+             << ": unknown element " << tok << endl;
+        return false;
+      }
+    }
+    if (!comment.empty() && comment.back() == '\r') comment.pop_back();
+    frames.push_back(std::move(mol));
+    comments.push_back(comment);
+  }
+  Natoms = frames.empty() ? 0 : (int)frames.back().size();
+  open_without_problems = !frames.empty();
+  return open_without_problems;
+}
+
 bool ReadXYZFile::GetValuesFromFile(string filename, vector<Atom>& molecule) {
   std::ifstream f(filename.c_str());
   if (!f.good()) {

@@ -48,6 +48,9 @@ class ReadXYZFile {
   int Natoms;
   bool open_without_problems;
   bool GetValuesFromFile(string, vector<Atom>&);
+  // Every frame of a multi-frame XYZ file (blocks of count line, comment line, atoms, one after
+  // the other; blank lines between blocks allowed) with its comment line.  Not in the reference.
+  bool GetFramesFromFile(string, vector<vector<Atom>>&, vector<string>&);
 };
 
 // ---- atomicOrbitals.h -------------------------------------------------------------------

@@ -87,3 +87,19 @@ def test_bond_geometry():
         C, H = m.xyz[m.Z == 6], m.xyz[m.Z == 1]
         dmin = np.min(np.linalg.norm(H[:, None] - C[None], axis=2), axis=1)
         assert np.all((dmin > 1.07) & (dmin < 1.10))
+
+
+def test_cli_frames_rejects_a_truncated_frame(tmp_path):
+    """The CLI's multi-frame reader (C++ façade) stops at a frame with fewer atom lines than its
+    count, before any device work."""
+    import subprocess
+
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "semigpu_b200", "semiGPU")
+    if not os.path.exists(cli):
+        pytest.skip("CLI not built")
+    p = tmp_path / "bad.xyz"
+    p.write_text("3\nwater\nO 0 0 0\nH 0.96 0 0\nH -0.24 0.93 0\n\n2\ncut\nH 0 0 0\n")
+    r = subprocess.run([cli, "--frames", str(p)], capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0
+    assert "frame 1" in r.stdout and "ends after 1 of 2 atoms" in r.stdout

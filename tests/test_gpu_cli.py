@@ -51,3 +51,27 @@ def test_cli_rejects_unsupported_element(tmp_path):
     r = subprocess.run([CLI, str(xyz)], capture_output=True, text=True, timeout=120)
     assert r.returncode != 0
     assert "MNDO parameters" in r.stdout + r.stderr
+
+
+def test_cli_frames_one_batch_against_oracle(tmp_path, oracle_mod):
+    """--frames --json: every frame of a multi-frame file (the golden CLI molecules, blank lines
+    between some frames) in one batched launch; each frame's energies and step count as the
+    oracle's."""
+    names = sorted(GOLD)
+    text = "\n".join(GOLD[n]["xyz"].strip() + ("\n" if i % 2 else "") for i, n in enumerate(names))
+    xyz = tmp_path / "ensemble.xyz"
+    xyz.write_text(text + "\n")
+    r = subprocess.run([CLI, "--tol", "1e-6", "--frames", "--json", "--heat", str(xyz)],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rows = [json.loads(line) for line in r.stdout.splitlines()]
+    assert [row["frame"] for row in rows] == list(range(len(names)))
+    from semigpu_b200 import geometry as geo
+
+    for row, n in zip(rows, names):
+        mol = geo.parse_xyz(GOLD[n]["xyz"])
+        o = oracle_mod.scf(mol.Z, mol.xyz, tol=1e-6)
+        assert row["natoms"] == mol.natoms and row["status"] == 0 and row["converged"]
+        assert row["n_iter"] == o["n_iter"], n
+        assert abs(row["E_tot"] - o["E_tot"]) < 1e-6, n
+        assert "heat_of_formation_kcal_mol" in row
