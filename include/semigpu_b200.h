@@ -136,6 +136,12 @@ int sgb_diag_barrier_timeout(sgb_ctx *ctx, int blocks, int extra, long long spin
  * synchronises the whole device, which would stall other contexts' work).  One batch at a time
  * uses the arena; bytes = 0 releases it. */
 int sgb_ctx_reserve(sgb_ctx *ctx, size_t bytes);
+/* Launch priority of the context's work: high != 0 puts its streams at the device's greatest
+ * stream priority, 0 at the default.  When the SMs are busy with another context's long
+ * persistent launches, the hardware then hands this context's blocks to the next free SMs
+ * before the other launches' waiting blocks (a serving loop gives its small-molecule workers
+ * high priority).  Waits for the context's queued work, then replaces its streams. */
+int sgb_ctx_set_priority(sgb_ctx *ctx, int high);
 /* Bytes of device memory currently held by the context: its molecules and batches, and the
  * arenas of destroyed ones that it keeps for reuse (at most 16 of them and 8 GiB; released
  * when the budget or a failed allocation needs the room, and by sgb_ctx_destroy). */

@@ -72,6 +72,7 @@ SIGNATURES = {
     "sgb_run_molecules": (ctypes.c_int, [_VP, ctypes.c_int, _I, _I, _D, ctypes.c_double,
                                          ctypes.c_int, _D, _D, _I, _I, _I]),
     "sgb_batch_last_ms": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_float)]),
+    "sgb_ctx_set_priority": (ctypes.c_int, [_VP, ctypes.c_int]),
     "sgb_gradient": (ctypes.c_int, [_VP, ctypes.c_int, _I, _D, ctypes.c_double, ctypes.c_int,
                                     ctypes.c_double, _D, _D]),
     "sgb_batch_launches": (ctypes.c_int, [_VP, _I]),
@@ -188,6 +189,11 @@ class Context:
         """CTA size per size class for this context's batched launches (see size_classes)."""
         t = np.ascontiguousarray(threads, np.int32)
         self.check(lib().sgb_ctx_set_class_threads(self.h, len(t), _i(t)), "set_class_threads")
+
+    def set_priority(self, high: bool = True):
+        """Launches of this context at the device's greatest stream priority (or the default):
+        its blocks go to freed SMs before other contexts' waiting blocks."""
+        self.check(lib().sgb_ctx_set_priority(self.h, int(bool(high))), "sgb_ctx_set_priority")
 
     def set_diis(self, depth: int):
         """Pulay DIIS of this depth (2..8; 0 = off) for this context's SCF runs (batched

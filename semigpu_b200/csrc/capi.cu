@@ -1681,6 +1681,29 @@ int sgb_ctx_set_sm_share(sgb_ctx* ctx, double share) {
   return SGB_OK;
 }
 
+int sgb_ctx_set_priority(sgb_ctx* ctx, int high) {
+  if (!ctx) return SGB_E_ARG;
+  int least = 0, greatest = 0;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  CUDA_TRY(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  const int prio = high ? greatest : least;
+  // every launch and copy of the context reads ctx->stream / ctx->aux[] when it is issued, so
+  // the streams can be replaced once the work queued on them has finished
+  cudaStream_t* all[1 + kNumClasses];
+  all[0] = &ctx->stream;
+  for (int k = 0; k < kNumClasses; ++k) all[1 + k] = &ctx->aux[k];
+  for (cudaStream_t* sp : all) {
+    cudaStream_t fresh = nullptr;
+    CUDA_TRY(ctx, cudaStreamCreateWithPriority(&fresh, cudaStreamNonBlocking, prio));
+    if (*sp) {
+      cudaStreamSynchronize(*sp);
+      cudaStreamDestroy(*sp);
+    }
+    *sp = fresh;
+  }
+  return SGB_OK;
+}
+
 int sgb_ctx_reserve(sgb_ctx* ctx, size_t bytes) {
   if (!ctx) return SGB_E_ARG;
   if (ctx->pool_busy) return fail(ctx, SGB_E_STATE, "the reserved arena is in use by a batch");

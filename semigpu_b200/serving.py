@@ -169,6 +169,9 @@ class Server:
                     ctx.set_diis(self.diis)
                 if big and self.big_slots:
                     ctx.set_sm_share(max(0.05, self.big_sm_share / self.big_slots))
+                elif self.big_slots:
+                    # small batches take freed SMs ahead of the large launches' waiting blocks
+                    ctx.set_priority(True)
                 # batches are built in a per-worker arena: no cudaMalloc/cudaFree per batch
                 # (cudaFree would synchronise the device and stall the other workers)
                 ctx.reserve(self.slot_budget + (64 << 20))

@@ -68,3 +68,18 @@ def test_batch_rerun_new_coordinates(gpu_ctx, oracle_mod):
         assert abs(r2["E_tot"][i] - o["E_tot"]) < 1e-6
     assert not np.allclose(r1["E_tot"], r2["E_tot"])
     assert b.last_ms() > 0
+
+
+def test_high_priority_context_same_results(gpu_ctx):
+    """sgb_ctx_set_priority replaces the context's streams; a batch on the high-priority streams
+    (and again after going back to the default) gives the default context's results."""
+    mols = geo.batch_c3(64, seed=5)
+    ref = sg.run_molecules(gpu_ctx, mols, tol=1e-6)
+    with sg.Context(0) as ctx:
+        ctx.set_priority(True)
+        hi = sg.run_molecules(ctx, mols, tol=1e-6)
+        ctx.set_priority(False)
+        lo = sg.run_molecules(ctx, mols, tol=1e-6)
+    for r in (hi, lo):
+        assert np.array_equal(r["n_iter"], ref["n_iter"])
+        assert np.max(np.abs(r["E_tot"] - ref["E_tot"])) == 0.0
