@@ -61,6 +61,7 @@ class Request:
     rid: int
     mol: Geometry
     t_arrival: float
+    t_submit: float = 0.0  # when submit() ran (replay() sets t_arrival to the scheduled time)
     t_start: float = 0.0
     t_done: float = 0.0
     result: dict = field(default_factory=dict)
@@ -106,7 +107,8 @@ class Server:
         with self._cv:
             rid = self._next
             self._next += 1
-            req = Request(rid, mol, time.perf_counter() if t_arrival is None else t_arrival)
+            now = time.perf_counter()
+            req = Request(rid, mol, now if t_arrival is None else t_arrival, t_submit=now)
             self._queues[int(self.big_slots > 0 and mol.nao > SMEM_MAX_NAO)].append(req)
             self._cv.notify_all()
         return rid
@@ -245,6 +247,10 @@ def stats(done: list[Request]) -> dict:
                 1e3 * float(np.percentile(lat[quarter == k], 50)) if np.any(quarter == k) else None
                 for k in range(4)],
             "drain_ms": 1e3 * (t_last - t_last_arrival),
+            # how late the replay submitted requests against their schedule (host-side lag that
+            # the latencies above include)
+            "submit_lag_p99_ms": 1e3 * float(np.percentile(
+                [max(0.0, r.t_submit - r.t_arrival) if r.t_submit else 0.0 for r in done], 99)),
             "all_converged": bool(all(r.result.get("converged", False) for r in done))}
 
 
