@@ -32,6 +32,7 @@ extern "C" {
 #define SGB_E_UNSUPPORTED -6  /* size outside what this build handles                        */
 #define SGB_E_EIG 1           /* SCF stopped: eigensolver did not converge (as LAPACK info>0)*/
 #define SGB_E_NAN 2           /* SCF stopped: non-finite energy                              */
+#define SGB_E_NOCONV 3        /* sgb_gradient: a geometry's SCF reached max_iter unconverged */
 
 /* ---- matrices that can be read back ----------------------------------------------------- */
 #define SGB_BLOCKS 0  /* integral blocks, the reference's ragged [A][B<=A] array flattened   */
@@ -245,7 +246,9 @@ int sgb_run_molecules(sgb_ctx *ctx, int nmol, const int *natoms, const int *Z, c
  * order of xyz), by central differences: the molecule and its 6 natoms copies displaced by
  * +/- step Angstrom along each coordinate run as one batch (one CTA per geometry, nao <= 1024);
  * *e_tot (may be NULL) receives the undisplaced total energy.  The SCF tolerance sets the
- * noise: about tol / step (use tol near 1e-9 eV with step 1e-4 Angstrom).  No counterpart in
+ * noise: about tol / step (use tol near 1e-9 eV with step 1e-4 Angstrom).  Any geometry whose
+ * SCF stops (SGB_E_EIG, SGB_E_NAN) or reaches max_iter unconverged (SGB_E_NOCONV) fails the
+ * call, and grad is then not written.  No counterpart in
  * the reference, whose README lists a geometry optimizer as future work (README.md:110). */
 int sgb_gradient(sgb_ctx *ctx, int natoms, const int *Z, const double *xyz, double tol,
                  int max_iter, double step, double *e_tot, double *grad);

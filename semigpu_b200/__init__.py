@@ -21,8 +21,8 @@ from . import geometry
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsemigpu_b200.so")
 
-OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN = (
-    0, -1, -2, -3, -4, -5, -6, 1, 2)
+OK, E_ARG, E_ELEMENT, E_CUDA, E_NOMEM, E_STATE, E_UNSUPPORTED, E_EIG, E_NAN, E_NOCONV = (
+    0, -1, -2, -3, -4, -5, -6, 1, 2, 3)
 BLOCKS, HCORE, FOCK, DENSITY, EIGVAL, EIGVEC = range(6)
 PATH_AUTO, PATH_CTA, PATH_GRID = range(3)
 SOLVER_PURIFY, SOLVER_JACOBI, SOLVER_PURIFY_MIXED = range(3)
@@ -457,8 +457,11 @@ def gradient(ctx: Context, mol, tol: float = 1e-9, max_iter: int = 200, step: fl
     xyz = np.ascontiguousarray(mol.xyz, np.float64).reshape(-1)
     g = np.zeros_like(xyz)
     e = ctypes.c_double()
-    ctx.check(lib().sgb_gradient(ctx.h, len(Z), _i(Z), _d(xyz), tol, max_iter, step,
-                                 ctypes.byref(e), _d(g)), "sgb_gradient")
+    rc = lib().sgb_gradient(ctx.h, len(Z), _i(Z), _d(xyz), tol, max_iter, step, ctypes.byref(e),
+                            _d(g))
+    if rc != 0:  # the SCF statuses (a geometry that stopped or did not converge) are positive
+        raise SGBError(rc, f"sgb_gradient: {lib().sgb_status_string(rc).decode()}: "
+                           f"{lib().sgb_last_error(ctx.h).decode()}")
     return e.value, g.reshape(-1, 3)
 
 

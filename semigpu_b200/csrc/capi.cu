@@ -1487,6 +1487,7 @@ const char* sgb_status_string(int s) {
     case SGB_E_UNSUPPORTED: return "unsupported size";
     case SGB_E_EIG: return "eigensolver did not converge";
     case SGB_E_NAN: return "non-finite energy";
+    case SGB_E_NOCONV: return "SCF did not converge within max_iter";
     default: return "unknown status";
   }
 }
@@ -2093,8 +2094,12 @@ int sgb_gradient(sgb_ctx* ctx, int natoms, const int* Z, const double* xyz, doub
   free_batch(b);
   if (rc) return rc;
   for (int m = 0; m < nmol; ++m) {
-    if (st[m] != MOL_OK) return st[m] == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN;
-    if (!cv[m]) return fail(ctx, SGB_E_EIG, "gradient: SCF of geometry %d did not converge", m);
+    if (st[m] != MOL_OK)
+      return fail(ctx, st[m] == MOL_EIG_FAILED ? SGB_E_EIG : SGB_E_NAN,
+                  "gradient: SCF of geometry %d stopped (status %d)", m, st[m]);
+    if (!cv[m])
+      return fail(ctx, SGB_E_NOCONV, "gradient: SCF of geometry %d did not converge in %d steps", m,
+                  max_iter);
   }
   if (e_tot) *e_tot = eel[0] + ecc[0];
   for (int64_t c = 0; c < per; ++c) {

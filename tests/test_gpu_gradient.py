@@ -63,6 +63,22 @@ def test_gradient_argument_errors(ctx):
         sg.gradient(ctx, mol, max_iter=0)
 
 
+def test_gradient_reports_scf_failures(ctx):
+    """A displaced geometry whose SCF reaches the step cap (SGB_E_NOCONV), or a non-finite
+    coordinate (SGB_E_NAN), fails the call instead of returning a gradient."""
+    mol = CASES["hexane"]
+    with pytest.raises(sg.SGBError) as info:
+        sg.gradient(ctx, mol, max_iter=2)
+    assert info.value.code == sg.E_NOCONV
+    bad = geo.Molecule(mol.Z, np.where(np.arange(mol.xyz.size).reshape(-1, 3) == 4, np.nan,
+                                       mol.xyz))
+    with pytest.raises(sg.SGBError) as info:
+        sg.gradient(ctx, bad)
+    assert info.value.code == sg.E_NAN
+    e, _ = sg.gradient(ctx, mol)  # the context is still usable
+    assert np.isfinite(e)
+
+
 def test_optimizer_on_device_lowers_the_energy(ctx):
     mol = CASES["formaldehyde"]
     e0, _ = sg.gradient(ctx, mol)
