@@ -610,8 +610,12 @@ def main():
     if rc is not None:
         sys.exit(rc)
     if args.probe_ranks:
-        print(json.dumps({"rank": env_int("RANK", 0), "world": env_int("WORLD_SIZE", 1),
-                          "local_rank": env_int("LOCAL_RANK", 0), "gpus": args.gpus}), flush=True)
+        # one write per line: the ranks share the launcher's stdout, and a line written in one
+        # call below the pipe's atomic size never interleaves with another rank's
+        line = json.dumps({"rank": env_int("RANK", 0), "world": env_int("WORLD_SIZE", 1),
+                           "local_rank": env_int("LOCAL_RANK", 0), "gpus": args.gpus}) + "\n"
+        sys.stdout.flush()
+        os.write(sys.stdout.fileno(), line.encode())
         return
     if args.impl == "reference":
         run_reference_arm(args)

@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import json
 import os
+import re
 import subprocess
 import sys
 
@@ -22,7 +23,7 @@ def test_gpus_two_starts_two_ranks():
     r = subprocess.run([sys.executable, BENCH, "--gpus", "2", "--probe-ranks"],
                        capture_output=True, text=True, timeout=300, env=_env())
     assert r.returncode == 0, r.stderr[-2000:]
-    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    lines = [json.loads(x) for x in re.findall(r"\{[^{}]*\}", r.stdout)]
     assert sorted(x["rank"] for x in lines) == [0, 1]
     assert all(x["world"] == 2 and x["gpus"] == 2 for x in lines)
     assert sorted(x["local_rank"] for x in lines) == [0, 1]
