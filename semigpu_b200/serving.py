@@ -37,6 +37,9 @@ from .geometry import Molecule as Geometry
 
 CTA_MAX_NAO = 1024  # larger molecules take the grid path
 SMEM_MAX_NAO = 160  # above this a batched molecule also holds its work matrices in global memory
+# nao 129-160: the largest shared-memory class, one CTA of ~225 KB shared memory, which starts
+# only on an SM with nothing else resident
+WHOLE_SM_NAO = 128
 
 
 def device_bytes(mol: Geometry, diis: int = 0) -> int:
@@ -71,14 +74,18 @@ class Server:
     def __init__(self, device: int = 0, slots: int = 3, max_batch: int = 4096,
                  hbm_budget: int = 16 << 30, tol: float = 1e-6, max_iter: int = 100,
                  batch_window_s: float = 0.0, engine=None, big_slots: int = 1,
-                 big_sm_share: float = 0.95, solver: int | None = None, diis: int = 0):
+                 big_sm_share: float = 0.95, solver: int | None = None, diis: int = 0,
+                 mid_slots: int = 0):
         """engine(ctx, mols, tol, max_iter) -> dict of arrays (defaults to run_molecules);
         replaceable for host-only tests of the scheduling.  big_slots of the slots serve the
         queue of molecules above nao 160 (at least one slot stays with the small queue); their
         launches together use at most big_sm_share of the SMs, so the persistent large-molecule
         launches (seconds) always leave SMs to the small ones.  solver: the density solver of
         every worker context (None: the library default); diis: DIIS depth of every worker
-        context (0: off)."""
+        context (0: off).  mid_slots of the slots (taken from the small ones, at least one
+        small slot stays) serve a third queue, molecules of nao 129-160: their CTA needs a whole
+        SM, and while the large launches hold most SMs it can wait for one for as long as a
+        large batch runs; in their own queue they no longer hold up the other small requests."""
         self.solver = solver
         self.diis = diis
         self.big_sm_share = big_sm_share
@@ -87,16 +94,24 @@ class Server:
         self.slot_budget = hbm_budget // max(1, slots)
         self.window = batch_window_s
         self.engine = engine or run_molecules
-        self._queues = (collections.deque(), collections.deque())  # small, large
+        self._queues = (collections.deque(), collections.deque(), collections.deque())
+        # small, large, whole-SM (nao 129-160)
         self.big_slots = max(0, min(big_slots, slots - 1))
+        self.mid_slots = max(0, min(mid_slots, slots - self.big_slots - 1))
         self._cv = threading.Condition()
         self._done: list[Request] = []
         self._next = 0
         self._stop = False
         self._device = device
-        # the last big_slots workers serve the large queue
-        self._workers = [threading.Thread(target=self._work, args=(i, i >= slots - self.big_slots),
-                                          daemon=True) for i in range(slots)]
+        # the last big_slots workers serve the large queue, the mid_slots before them the
+        # whole-SM one
+        def kind(i):
+            if i >= slots - self.big_slots:
+                return 1
+            return 2 if i >= slots - self.big_slots - self.mid_slots else 0
+
+        self._workers = [threading.Thread(target=self._work, args=(i, kind(i)), daemon=True)
+                         for i in range(slots)]
         self.batches: list[tuple[int, int, float, float]] = []  # (worker, size, t0, t1)
         self._errors: list[BaseException] = []
         for w in self._workers:
@@ -109,7 +124,13 @@ class Server:
             self._next += 1
             now = time.perf_counter()
             req = Request(rid, mol, now if t_arrival is None else t_arrival, t_submit=now)
-            self._queues[int(self.big_slots > 0 and mol.nao > SMEM_MAX_NAO)].append(req)
+            if self.big_slots > 0 and mol.nao > SMEM_MAX_NAO:
+                q = 1
+            elif self.mid_slots > 0 and mol.nao > WHOLE_SM_NAO:
+                q = 2
+            else:
+                q = 0
+            self._queues[q].append(req)
             self._cv.notify_all()
         return rid
 
@@ -159,8 +180,9 @@ class Server:
             out.append(queue.popleft())
         return out
 
-    def _work(self, idx: int, big: bool = False):
-        queue = self._queues[int(big)]
+    def _work(self, idx: int, kind: int = 0):
+        queue = self._queues[kind]
+        big = kind == 1
         ctx = None
         try:
             if self.engine is run_molecules:
@@ -272,6 +294,8 @@ def main(argv=None):
     ap.add_argument("--duration", type=float, default=3.0, help="seconds of arrivals")
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--big-slots", type=int, default=2)
+    ap.add_argument("--mid-slots", type=int, default=0,
+                    help="workers of their own for nao 129-160 (whole-SM CTAs)")
     ap.add_argument("--hbm-gb", type=float, default=40.0)
     ap.add_argument("--big-share", type=float, default=0.95,
                     help="fraction of the SMs the large-molecule workers' launches may use")
@@ -291,7 +315,8 @@ def main(argv=None):
                 break
             times.append(t)
         arrivals = list(zip(times, geo.batch_c3(len(times), seed=args.seed)))
-    srv = Server(slots=args.slots, big_slots=args.big_slots, hbm_budget=int(args.hbm_gb * (1 << 30)),
+    srv = Server(slots=args.slots, big_slots=args.big_slots, mid_slots=args.mid_slots,
+                 hbm_budget=int(args.hbm_gb * (1 << 30)),
                  big_sm_share=args.big_share,
                  solver=SOLVER_PURIFY_MIXED if args.mixed else SOLVER_PURIFY, diis=args.diis)
     try:

@@ -71,6 +71,40 @@ def test_small_and_large_molecules_never_share_a_batch():
     assert any(all(n > serving.SMEM_MAX_NAO for n in b) for b in batches)
 
 
+def test_whole_sm_molecules_have_their_own_queue():
+    """With mid_slots, molecules of nao 129-160 (whole-SM CTAs) go to their own worker: no
+    batch mixes them with smaller or larger molecules."""
+    batches = []
+    lock = threading.Lock()
+    inner = _fake_engine(delay=0.003)
+
+    def engine(ctx, mols, tol, max_iter):
+        with lock:
+            batches.append([m.nao for m in mols])
+        return inner(ctx, mols, tol, max_iter)
+
+    rng = np.random.default_rng(8)
+    mid = [geo.alkane(int(k), rng) for k in (22, 24, 26)]  # nao 134, 146, 158
+    assert all(serving.WHOLE_SM_NAO < m.nao <= serving.SMEM_MAX_NAO for m in mid)
+    mols = geo.batch_c3(90, seed=7) + mid + [geo.alkane(int(k), rng) for k in (30, 45)]
+    order = rng.permutation(len(mols))
+    srv = serving.Server(slots=4, big_slots=1, mid_slots=1, engine=engine)
+    try:
+        for i in order:
+            srv.submit(mols[i])
+        done = srv.drain(timeout=60)
+    finally:
+        srv.close()
+    assert len(done) == len(mols)
+
+    def kind(n):
+        return 1 if n > serving.SMEM_MAX_NAO else 2 if n > serving.WHOLE_SM_NAO else 0
+
+    for b in batches:
+        assert len({kind(n) for n in b}) == 1, b
+    assert any(kind(b[0]) == 2 for b in batches)
+
+
 def test_admission_respects_hbm_share():
     log = []
     mols = geo.batch_c3(50, seed=3)
